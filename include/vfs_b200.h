@@ -1,0 +1,126 @@
+/*
+ * vfs_b200 — C ABI of the B200 variational fisheye stereo (TGV-L1) solver.
+ *
+ * Every function returns an int status: VFS_OK (0) or a negative VFS_ERR_* code;
+ * nothing in the library exits the process.  vfs_status_string() names a code and
+ * vfs_last_error() returns the message of the last failure on a handle.
+ *
+ * Threading: a handle must be used by one host thread at a time.  All device work
+ * of a handle is ordered on its CUDA stream (vfs_set_stream); host-buffer entry
+ * points synchronise that stream before they return, device-pointer entry points do
+ * not.
+ *
+ * Images, masks and vector fields are tightly packed row-major width x height arrays
+ * (2 interleaved floats per pixel for vector fields), the raw-pointer equivalent of the
+ * cv::Mat arguments of the reference class.
+ */
+#ifndef VFS_B200_H
+#define VFS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VFS_OK 0
+#define VFS_ERR_ARG (-1)      /* invalid argument or size */
+#define VFS_ERR_CUDA (-2)     /* a CUDA runtime call failed */
+#define VFS_ERR_STATE (-3)    /* call order violated (e.g. solve before initialize) */
+#define VFS_ERR_NOMEM (-4)    /* device allocation failed */
+#define VFS_ERR_IO (-5)       /* file could not be read or parsed */
+#define VFS_ERR_TIMEOUT (-6)  /* a device-side wait ran out of iterations */
+#define VFS_ERR_BUSY (-7)     /* admission refused: not enough free device memory */
+
+typedef struct vfs_stereo vfs_stereo;
+
+const char* vfs_status_string(int status);
+const char* vfs_last_error(const vfs_stereo* s);
+int vfs_version(void); /* 100 * major + minor */
+
+/* StereoTgv::StereoTgv() (stereotgv/stereotgv.cu:32-36; dllhook/vfs.cpp:3-6 Create). */
+int vfs_create(vfs_stereo** out);
+/* StereoTgv::StereoTgv(blockWidth, blockHeight, strideAlignment) (stereotgv.cu:38-42).
+ * strideAlignment sets the row pitch in elements; blockWidth sets the column extent of
+ * the reference's tensor launch (calcTensor.cu:81,227). */
+int vfs_create_ex(vfs_stereo** out, int blockWidth, int blockHeight, int strideAlignment);
+int vfs_destroy(vfs_stereo* s);
+/* Select the CUDA stream (a cudaStream_t) used for all device work of the handle. */
+int vfs_set_stream(vfs_stereo* s, void* cuda_stream);
+int vfs_synchronize(vfs_stereo* s);
+
+/* StereoTgv::initialize (stereotgv/stereotgv.h:107-109, stereotgv.cu:44-168). */
+int vfs_initialize(vfs_stereo* s, int width, int height, float beta, float gamma, float alpha0,
+                   float alpha1, float timestep_lambda, float lambda, int nLevels, float fScale,
+                   int nWarpIters, int nSolverIters);
+/* Public fields of the reference class: limitRange (stereotgv.h:45, default 1.0),
+ * baseline / focal (stereotgv.h:31-32, set by dllhook/vfs.cpp:15-16). */
+int vfs_set_limit_range(vfs_stereo* s, float limit_range);
+int vfs_set_camera(vfs_stereo* s, float baseline, float focal);
+/* Pyramid geometry of an initialized handle: level sizes and pitches (elements). */
+int vfs_get_level_size(const vfs_stereo* s, int level, int* width, int* height, int* stride);
+
+/* StereoTgv::loadVectorFields(translation, calibration) (stereotgv.h:110,
+ * stereotgv.cu:171-199): two H x W x 2 float32 fields in host memory. */
+int vfs_load_vector_fields(vfs_stereo* s, const float* translation, const float* calibration);
+/* StereoTgv::copyMaskToDevice (stereotgv.h:115, stereotgv.cu:241-252): H x W float32, 0 = off. */
+int vfs_copy_mask_to_device(vfs_stereo* s, const float* mask);
+
+/* StereoTgv::copyImagesToDevice(uchar*, uchar*) (stereotgv.h:112, stereotgv.cu:201-213). */
+int vfs_copy_images_to_device_u8(vfs_stereo* s, const uint8_t* i0, const uint8_t* i1);
+/* StereoTgv::copyImagesToDevice(cv::Mat, cv::Mat) for CV_32F and CV_8UC3 (stereotgv.cu:215-239). */
+int vfs_copy_images_to_device_f32(vfs_stereo* s, const float* i0, const float* i1);
+int vfs_copy_images_to_device_u8c3(vfs_stereo* s, const uint8_t* i0_rgb, const uint8_t* i1_rgb);
+/* Same as the u8 copy with the images already in device memory (tight W x H); stream-ordered. */
+int vfs_copy_images_from_device_u8(vfs_stereo* s, const uint8_t* d_i0, const uint8_t* d_i1);
+
+/* StereoTgv::solveStereoForward / solveStereoForwardMasked (stereotgv.h:116-117,
+ * stereotgv.cu:256-387 and 389-515).  Stream-ordered: returns after enqueueing. */
+int vfs_solve_stereo_forward(vfs_stereo* s);
+int vfs_solve_stereo_forward_masked(vfs_stereo* s);
+
+/* StereoTgv::copy1DDisparityToHost (stereotgv.cu:533-540): W x H float32. */
+int vfs_copy_1d_disparity_to_host(vfs_stereo* s, float* u);
+/* StereoTgv::copyDisparityToHost (stereotgv.cu:542-549): W x H x 2 float32. */
+int vfs_copy_disparity_to_host(vfs_stereo* s, float* warp_uv);
+/* StereoTgv::copyWarpedImageToHost (stereotgv.cu:561-568): W x H float32. */
+int vfs_copy_warped_image_to_host(vfs_stereo* s, float* image);
+/* Device-pointer outputs (tight W x H / W x H x 2), stream-ordered. */
+int vfs_copy_1d_disparity_to_device(vfs_stereo* s, float* d_u);
+int vfs_copy_disparity_to_device(vfs_stereo* s, float* d_warp_uv);
+/* StereoTgv::copyStereoToHost (stereotgv.h:118-120, stereotgv.cu:517-531; kernel
+ * conversion.cu:3-69): depth W x H and X W x H x 3 from the 2-D disparity, with the
+ * reference's argument order (focalx, focaly, cx, cy, d1..d4, t1..t3). */
+int vfs_copy_stereo_to_host(vfs_stereo* s, float* depth, float* X, float focalx, float focaly,
+                            float cx, float cy, float d1, float d2, float d3, float d4, float t1,
+                            float t2, float t3);
+/* StereoTgv::copyDisparityVisToHost (stereotgv.cu:551-559; flowToHsv.cu:4-110): W x H x 3. */
+int vfs_copy_disparity_vis_to_host(vfs_stereo* s, float* rgb, float flow_scale);
+
+/* Inspection of internal state for tests: copy the level-0 view (W x H x comps) of a
+ * named solver buffer ("u", "u_", "warpUV", "a", "b", "c", "etau", "Iu", "Iz", "i1warp",
+ * "tv2", "p", "q", "Tp", ...) to host memory. */
+int vfs_debug_get_buffer(vfs_stereo* s, const char* name, int comps, float* out);
+
+/* ---- reference DLL entry points (dllhook/vfs.h:37-44) -------------------------------
+ * Create / Init / SolveStereo with the reference's names and argument lists.  Init reads
+ * the mask (8-bit PNG or binary PGM, scaled by 1/255) and the two Middlebury .flo fields.
+ * SolveStereo equalises both images' histograms on the device (the reference calls
+ * cv::equalizeHist), solves the masked problem and, unlike the reference (which leaves
+ * it unwritten, dllhook/vfs.cpp:42-47), fills `output` with depth8 = clamp(255 * Z /
+ * maxDepth) using the focal/baseline set by Init.  Errors are reported by
+ * vfs_last_error() on the handle. */
+vfs_stereo* Create(void);
+void Init(vfs_stereo* vfs, int stereoWidth, int stereoHeight, float beta, float gamma,
+          float alpha0, float alpha1, float timeStepLambda, float lambda, int nLevel,
+          float fScale, int nWarpIters, int nSolverIters, float focal, float baseline,
+          const char* fisheyeMaskFilename, const char* translationVectorFilename,
+          const char* calibrationVectorFilename);
+void SolveStereo(vfs_stereo* vfs, unsigned char* fs1, unsigned char* fs2, unsigned char* output,
+                 int stereoWidth, int stereoHeight, float maxDepth);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VFS_B200_H */

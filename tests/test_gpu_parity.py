@@ -1,0 +1,87 @@
+"""CUDA drop-in path (through the C ABI) against the CPU oracle on the same inputs.
+
+Tolerances: the float32 oracle restates the reference kernels with the same operation
+order as the CUDA kernels, so the two agree to float32 rounding of the few library
+functions (expf, powf) and of rare texture-filter ties: max |du| <= 1e-3 px (the drop-in
+bar).  Against the float64 oracle (the method in double precision) the mean disparity
+error must stay <= 0.05 px.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from tests.helpers import diff_stats, params, random_case, run_gpu, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL_MAX_F32 = 1e-3
+TOL_MEAN_F64 = 0.05
+
+
+@pytest.mark.parametrize("masked", [True, False])
+@pytest.mark.parametrize("size", [(67, 53), (96, 64), (130, 101)])
+def test_small_random_cases(gpu, masked, size):
+    w, h = size
+    i0, i1, mask, tv, cv = random_case(w, h, seed=w * 7 + h)
+    p = params(n_levels=2, n_warp=2, n_iter=7)
+    s = run_gpu(i0, i1, mask, tv, cv, p, masked)
+    o = run_oracle(i0, i1, mask, tv, cv, p, masked, precision=32)
+    for name, comps in (("u", 1), ("warpUV", 2), ("u_", 1)):
+        st = diff_stats(s.debug_buffer(name, comps), o.get(name, comps))
+        assert st["max"] <= TOL_MAX_F32, (name, st)
+
+
+def test_single_level_intermediates(gpu):
+    # one level, one warp, one iteration: every intermediate is a single kernel deep
+    i0, i1, mask, tv, cv = random_case(80, 61, seed=3)
+    p = params(n_levels=1, n_warp=1, n_iter=1)
+    s = run_gpu(i0, i1, mask, tv, cv, p, True)
+    o = run_oracle(i0, i1, mask, tv, cv, p, True, precision=32)
+    for name, comps, tol in (("i1warp", 1, 0), ("Iz", 1, 0), ("Iu", 1, 1e-7), ("i0smooth", 1, 0),
+                             ("a", 1, 1e-6), ("b", 1, 1e-6), ("c", 1, 1e-6), ("etau", 1, 1e-5),
+                             ("p", 2, 1e-6), ("q", 4, 1e-6), ("u", 1, 1e-6), ("u_", 1, 1e-6), ("tv2", 2, 0)):
+        st = diff_stats(s.debug_buffer(name, comps), o.get(name, comps))
+        assert st["max"] <= tol, (name, st)
+
+
+def test_state_persists_across_frames(gpu):
+    # the reference keeps stale values in masked-out pixels between frames
+    i0, i1, mask, tv, cv = random_case(72, 60, seed=11)
+    p = params(n_levels=2, n_warp=2, n_iter=4)
+    s = run_gpu(i0, i1, mask, tv, cv, p, True, frames=3)
+    o = run_oracle(i0, i1, mask, tv, cv, p, True, precision=32, frames=3)
+    st = diff_stats(s.copy1DDisparityToHost(), o.get("u"))
+    assert st["max"] <= TOL_MAX_F32, st
+
+
+def test_wang_golden_config(gpu):
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "wang_half", "wang_half.npz"))
+    p = params(beta=9.0, gamma=0.85, n_levels=5, n_warp=20, n_iter=10, limit_range=0.1)
+    mask = d["mask_u8"].astype(np.float32) / 255.0
+    s = run_gpu(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True)
+    o32 = run_oracle(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True, precision=32)
+    m = mask > 0
+    u = s.copy1DDisparityToHost()
+    st = diff_stats(u, o32.get("u"), m)
+    assert st["mean"] <= 1e-4, st
+    o64 = run_oracle(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True, precision=64)
+    assert diff_stats(u, o64.get("u"), m)["mean"] <= TOL_MEAN_F64
+
+
+@pytest.mark.parametrize("wh", [(424, 400), (848, 800)])
+def test_synthetic_benchmark_configs(gpu, wh):
+    from vfs_b200 import synth
+    w, h = wh
+    pair = synth.make_pair(w, h, seed=1000 + w)
+    sp = synth.SOLVER_PARAMS
+    p = params(beta=sp["beta"], gamma=sp["gamma"], n_levels=synth.n_levels_for(w), n_warp=sp["nWarpIters"],
+               n_iter=sp["nSolverIters"], limit_range=synth.LIMIT_RANGE)
+    s = run_gpu(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True)
+    u = s.copy1DDisparityToHost()
+    m = pair.mask > 0
+    o32 = run_oracle(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True, precision=32)
+    st = diff_stats(u, o32.get("u"), m)
+    assert st["mean"] <= 1e-4 and st["p99"] <= TOL_MAX_F32, st
+    o64 = run_oracle(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True, precision=64)
+    assert diff_stats(u, o64.get("u"), m)["mean"] <= TOL_MEAN_F64

@@ -1,0 +1,313 @@
+// extern "C" layer over StereoTgvImpl (declarations in include/vfs_b200.h).
+// Every entry point converts exceptions into a status code and records the
+// message on the handle; nothing here exits the process.
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/vfs_b200.h"
+#include "hist.cuh"
+#include "io.hpp"
+#include "stereo_tgv.cuh"
+
+struct vfs_stereo {
+  vfs::StereoTgvImpl impl;
+  std::string err;
+  // SolveStereo scratch (device): 2 images, histogram and LUT
+  uint8_t* d_eq = nullptr;
+  unsigned int* d_hist = nullptr;
+  size_t eq_bytes = 0;
+  vfs_stereo(int bw, int bh, int sa) : impl(bw, bh, sa) {}
+  ~vfs_stereo() {
+    if (d_eq) cudaFree(d_eq);
+  }
+};
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class F>
+int guarded(vfs_stereo* s, F&& f) {
+  if (!s) return VFS_ERR_ARG;
+  try {
+    f();
+    return VFS_OK;
+  } catch (const vfs::CudaError& e) {
+    s->err = std::string("CUDA error ") + cudaGetErrorString(e.err) + " in " + e.what;
+    (void)cudaGetLastError();
+    return e.err == cudaErrorMemoryAllocation ? VFS_ERR_NOMEM : VFS_ERR_CUDA;
+  } catch (const vfs::ArgError& e) {
+    s->err = e.msg;
+    return VFS_ERR_ARG;
+  } catch (const std::bad_alloc&) {
+    s->err = "host allocation failed";
+    return VFS_ERR_NOMEM;
+  } catch (...) {
+    s->err = "unknown error";
+    return VFS_ERR_CUDA;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* vfs_status_string(int st) {
+  switch (st) {
+    case VFS_OK: return "ok";
+    case VFS_ERR_ARG: return "invalid argument";
+    case VFS_ERR_CUDA: return "CUDA error";
+    case VFS_ERR_STATE: return "invalid call order";
+    case VFS_ERR_NOMEM: return "out of device memory";
+    case VFS_ERR_IO: return "file error";
+    case VFS_ERR_TIMEOUT: return "device wait timed out";
+    case VFS_ERR_BUSY: return "not enough free device memory";
+    default: return "unknown status";
+  }
+}
+
+const char* vfs_last_error(const vfs_stereo* s) { return s ? s->err.c_str() : g_create_error.c_str(); }
+
+int vfs_version(void) { return 100; }
+
+int vfs_create_ex(vfs_stereo** out, int bw, int bh, int sa) {
+  if (!out) return VFS_ERR_ARG;
+  *out = nullptr;
+  if (bw <= 0 || bh <= 0 || sa <= 0) {
+    g_create_error = "vfs_create_ex: block and stride alignment must be positive";
+    return VFS_ERR_ARG;
+  }
+  vfs_stereo* s = new (std::nothrow) vfs_stereo(bw, bh, sa);
+  if (!s) return VFS_ERR_NOMEM;
+  *out = s;
+  return VFS_OK;
+}
+
+int vfs_create(vfs_stereo** out) { return vfs_create_ex(out, 32, 1, 32); }
+
+int vfs_destroy(vfs_stereo* s) {
+  if (!s) return VFS_ERR_ARG;
+  cudaStreamSynchronize(s->impl.stream());
+  delete s;
+  return VFS_OK;
+}
+
+int vfs_set_stream(vfs_stereo* s, void* st) {
+  return guarded(s, [&] { s->impl.setStream((cudaStream_t)st); });
+}
+
+int vfs_synchronize(vfs_stereo* s) {
+  return guarded(s, [&] { VFS_CUDA(cudaStreamSynchronize(s->impl.stream())); });
+}
+
+int vfs_initialize(vfs_stereo* s, int width, int height, float beta, float gamma, float alpha0, float alpha1,
+                   float timestep_lambda, float lambda, int nLevels, float fScale, int nWarpIters,
+                   int nSolverIters) {
+  return guarded(s, [&] {
+    vfs::SolverParams p;
+    p.width = width;
+    p.height = height;
+    p.beta = beta;
+    p.gamma = gamma;
+    p.alpha0 = alpha0;
+    p.alpha1 = alpha1;
+    p.timestep_lambda = timestep_lambda;
+    p.lambda = lambda;
+    p.nLevels = nLevels;
+    p.fScale = fScale;
+    p.nWarpIters = nWarpIters;
+    p.nSolverIters = nSolverIters;
+    p.limitRange = s->impl.P.limitRange;
+    s->impl.initialize(p);
+  });
+}
+
+int vfs_set_limit_range(vfs_stereo* s, float lr) {
+  return guarded(s, [&] { s->impl.P.limitRange = lr; });
+}
+
+int vfs_set_camera(vfs_stereo* s, float baseline, float focal) {
+  return guarded(s, [&] {
+    s->impl.baseline = baseline;
+    s->impl.focal = focal;
+  });
+}
+
+int vfs_get_level_size(const vfs_stereo* cs, int level, int* w, int* h, int* st) {
+  vfs_stereo* s = const_cast<vfs_stereo*>(cs);
+  return guarded(s, [&] {
+    if (!s->impl.initialized()) throw vfs::ArgError{"get_level_size before initialize"};
+    if (level < 0 || level >= (int)s->impl.pW.size()) throw vfs::ArgError{"level out of range"};
+    if (w) *w = s->impl.pW[level];
+    if (h) *h = s->impl.pH[level];
+    if (st) *st = s->impl.pS[level];
+  });
+}
+
+int vfs_load_vector_fields(vfs_stereo* s, const float* tv, const float* cv) {
+  return guarded(s, [&] { s->impl.loadVectorFields(tv, cv); });
+}
+
+int vfs_copy_mask_to_device(vfs_stereo* s, const float* mask) {
+  return guarded(s, [&] { s->impl.copyMaskToDevice(mask); });
+}
+
+int vfs_copy_images_to_device_u8(vfs_stereo* s, const uint8_t* i0, const uint8_t* i1) {
+  return guarded(s, [&] { s->impl.copyImagesU8(i0, i1, false); });
+}
+
+int vfs_copy_images_to_device_f32(vfs_stereo* s, const float* i0, const float* i1) {
+  return guarded(s, [&] { s->impl.copyImagesF32(i0, i1); });
+}
+
+int vfs_copy_images_to_device_u8c3(vfs_stereo* s, const uint8_t* i0, const uint8_t* i1) {
+  return guarded(s, [&] { s->impl.copyImagesU8C3(i0, i1); });
+}
+
+int vfs_copy_images_from_device_u8(vfs_stereo* s, const uint8_t* d0, const uint8_t* d1) {
+  return guarded(s, [&] { s->impl.copyImagesU8(d0, d1, true); });
+}
+
+int vfs_solve_stereo_forward(vfs_stereo* s) {
+  return guarded(s, [&] { s->impl.solve(false); });
+}
+
+int vfs_solve_stereo_forward_masked(vfs_stereo* s) {
+  return guarded(s, [&] { s->impl.solve(true); });
+}
+
+int vfs_copy_1d_disparity_to_host(vfs_stereo* s, float* u) {
+  return guarded(s, [&] { s->impl.copyOut("u", u, true); });
+}
+
+int vfs_copy_disparity_to_host(vfs_stereo* s, float* uv) {
+  return guarded(s, [&] { s->impl.copyOut("warpUV", uv, true); });
+}
+
+int vfs_copy_warped_image_to_host(vfs_stereo* s, float* im) {
+  return guarded(s, [&] { s->impl.copyOut("i1warp", im, true); });
+}
+
+int vfs_copy_1d_disparity_to_device(vfs_stereo* s, float* d_u) {
+  return guarded(s, [&] { s->impl.copyOut("u", d_u, false); });
+}
+
+int vfs_copy_disparity_to_device(vfs_stereo* s, float* d_uv) {
+  return guarded(s, [&] { s->impl.copyOut("warpUV", d_uv, false); });
+}
+
+int vfs_copy_stereo_to_host(vfs_stereo* s, float* depth, float* X, float fx, float fy, float cx, float cy, float d1,
+                            float d2, float d3, float d4, float t1, float t2, float t3) {
+  return guarded(s, [&] {
+    s->impl.convertKB(fx, fy, cx, cy, d1, d2, d3, d4, t1, t2, t3);
+    if (depth) s->impl.copyOut("depth", depth, true);
+    if (X) s->impl.copyOut("X", X, true);
+    VFS_CUDA(cudaStreamSynchronize(s->impl.stream()));
+  });
+}
+
+int vfs_copy_disparity_vis_to_host(vfs_stereo* s, float* rgb, float flow_scale) {
+  return guarded(s, [&] {
+    s->impl.flowToHSV(flow_scale);
+    s->impl.copyOut("rgb", rgb, true);
+  });
+}
+
+int vfs_debug_get_buffer(vfs_stereo* s, const char* name, int comps, float* out) {
+  return guarded(s, [&] {
+    if (!name || !out) throw vfs::ArgError{"debug get: null argument"};
+    s->impl.debugGet(name, comps, out);
+  });
+}
+
+// ---- reference DLL entry points (dllhook/vfs.cpp) --------------------------------
+vfs_stereo* Create(void) {
+  vfs_stereo* s = nullptr;
+  vfs_create(&s);
+  return s;
+}
+
+void Init(vfs_stereo* s, int w, int h, float beta, float gamma, float alpha0, float alpha1, float tsl, float lambda,
+          int nLevel, float fScale, int nWarpIters, int nSolverIters, float focal, float baseline,
+          const char* maskFile, const char* tvFile, const char* cvFile) {
+  guarded(s, [&] {
+    vfs::SolverParams p;
+    p.width = w;
+    p.height = h;
+    p.beta = beta;
+    p.gamma = gamma;
+    p.alpha0 = alpha0;
+    p.alpha1 = alpha1;
+    p.timestep_lambda = tsl;
+    p.lambda = lambda;
+    p.nLevels = nLevel;
+    p.fScale = fScale;
+    p.nWarpIters = nWarpIters;
+    p.nSolverIters = nSolverIters;
+    p.limitRange = s->impl.P.limitRange;
+    s->impl.initialize(p);
+    s->impl.baseline = baseline;
+    s->impl.focal = focal;
+    std::string err;
+    int mw, mh;
+    std::vector<uint8_t> m8;
+    if (!maskFile || !vfs::read_gray8(maskFile, mw, mh, m8, err)) throw vfs::ArgError{"Init: mask: " + err};
+    if (mw != w || mh != h) throw vfs::ArgError{"Init: mask size differs from the solver size"};
+    std::vector<float> mask((size_t)w * h);
+    for (size_t i = 0; i < mask.size(); i++) mask[i] = (float)(m8[i] * (1.0 / 255.0));  // convertTo(CV_32F, 1/255)
+    s->impl.copyMaskToDevice(mask.data());
+    int tw, th, cw, ch;
+    std::vector<float> tv, cv;
+    if (!tvFile || !vfs::read_flo(tvFile, tw, th, tv, err)) throw vfs::ArgError{"Init: translation field: " + err};
+    if (!cvFile || !vfs::read_flo(cvFile, cw, ch, cv, err)) throw vfs::ArgError{"Init: calibration field: " + err};
+    if (tw != w || th != h || cw != w || ch != h) throw vfs::ArgError{"Init: vector field size differs"};
+    s->impl.loadVectorFields(tv.data(), cv.data());
+  });
+}
+
+void SolveStereo(vfs_stereo* s, unsigned char* fs1, unsigned char* fs2, unsigned char* output, int w, int h,
+                 float maxDepth) {
+  guarded(s, [&] {
+    auto& I = s->impl;
+    if (!I.initialized()) throw vfs::ArgError{"SolveStereo before Init"};
+    if (!fs1 || !fs2) throw vfs::ArgError{"SolveStereo: null image"};
+    if (w != I.width || h != I.height) throw vfs::ArgError{"SolveStereo: image size differs from Init"};
+    size_t n = (size_t)w * h;
+    size_t need = 2 * n + 256 * sizeof(unsigned int) + 256 + 1024;
+    if (s->eq_bytes < need) {
+      if (s->d_eq) cudaFree(s->d_eq);
+      s->d_eq = nullptr;
+      VFS_CUDA(cudaMalloc(&s->d_eq, need));
+      s->eq_bytes = need;
+    }
+    uint8_t* e0 = s->d_eq;
+    uint8_t* e1 = s->d_eq + n;
+    unsigned int* hist = (unsigned int*)(s->d_eq + ((2 * n + 255) & ~(size_t)255));
+    uint8_t* lut = (uint8_t*)(hist + 256);
+    cudaStream_t st = I.stream();
+    VFS_CUDA(cudaMemcpyAsync(e0, fs1, n, cudaMemcpyHostToDevice, st));
+    VFS_CUDA(cudaMemcpyAsync(e1, fs2, n, cudaMemcpyHostToDevice, st));
+    vfs::launch_equalize_hist(e0, e0, n, hist, lut, st);
+    vfs::launch_equalize_hist(e1, e1, n, hist, lut, st);
+    I.copyImagesU8(e0, e1, true);
+    I.solve(true);
+    if (output) {
+      std::vector<float> u(n);
+      I.copyOut("u", u.data(), true);
+      // depth from the 1-D disparity with the focal length and baseline given to
+      // Init: Z = focal * |baseline| / u, written as round(255 * Z / maxDepth)
+      // clamped to 0..255 (0 where u <= 0).
+      for (size_t i = 0; i < n; i++) {
+        float z = u[i] > 0.0f ? I.focal * std::fabs(I.baseline) / u[i] : 0.0f;
+        float v = maxDepth > 0.0f ? 255.0f * z / maxDepth : 0.0f;
+        output[i] = (uint8_t)(v <= 0.0f ? 0 : v >= 255.0f ? 255 : (int)std::lround(v));
+      }
+    } else {
+      VFS_CUDA(cudaStreamSynchronize(st));
+    }
+  });
+}
+
+}  // extern "C"

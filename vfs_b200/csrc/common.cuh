@@ -1,0 +1,81 @@
+// Shared host/device helpers of the vfs_b200 library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <map>
+#include <string>
+#include <tuple>
+
+namespace vfs {
+
+// Error carried from a failing CUDA call to the C ABI as a status code.
+struct CudaError {
+  cudaError_t err;
+  const char* what;
+  const char* file;
+  int line;
+};
+
+#define VFS_CUDA(call)                                            \
+  do {                                                            \
+    cudaError_t e_ = (call);                                      \
+    if (e_ != cudaSuccess) throw ::vfs::CudaError{e_, #call, __FILE__, __LINE__}; \
+  } while (0)
+
+#define VFS_LAUNCH_CHECK() VFS_CUDA(cudaGetLastError())
+
+struct ArgError {
+  std::string msg;
+};
+
+inline int iDivUp(int n, int m) { return (n + m - 1) / m; }
+
+// Launch shape of the plain per-pixel kernels: 32 columns x 8 rows, so a warp reads
+// one row segment (coalesced for float, float2 and float4 rows).
+constexpr int kBX = 32;
+constexpr int kBY = 8;
+inline dim3 grid2d(int w, int h) { return dim3(iDivUp(w, kBX), iDivUp(h, kBY)); }
+inline dim3 block2d() { return dim3(kBX, kBY); }
+
+// Texture objects with the sampling setup of every gather of the reference
+// (normalized coordinates, mirror addressing, pitch-2D float / float2 memory).
+// Objects are created once per (pointer, geometry, filter) and kept for the life
+// of the cache, so a launch never creates or destroys one.
+class TexCache {
+ public:
+  ~TexCache() { clear(); }
+  cudaTextureObject_t get(const void* ptr, int w, int h, size_t pitchBytes, int comps, bool linear) {
+    Key k{(uintptr_t)ptr, w, h, pitchBytes, comps, linear};
+    auto it = map_.find(k);
+    if (it != map_.end()) return it->second;
+    cudaResourceDesc rd = {};
+    rd.resType = cudaResourceTypePitch2D;
+    rd.res.pitch2D.devPtr = const_cast<void*>(ptr);
+    rd.res.pitch2D.desc = comps == 2 ? cudaCreateChannelDesc<float2>() : cudaCreateChannelDesc<float>();
+    rd.res.pitch2D.width = w;
+    rd.res.pitch2D.height = h;
+    rd.res.pitch2D.pitchInBytes = pitchBytes;
+    cudaTextureDesc td = {};
+    td.addressMode[0] = cudaAddressModeMirror;
+    td.addressMode[1] = cudaAddressModeMirror;
+    td.filterMode = linear ? cudaFilterModeLinear : cudaFilterModePoint;
+    td.readMode = cudaReadModeElementType;
+    td.normalizedCoords = 1;
+    cudaTextureObject_t t = 0;
+    VFS_CUDA(cudaCreateTextureObject(&t, &rd, &td, nullptr));
+    map_[k] = t;
+    return t;
+  }
+  void clear() {
+    for (auto& kv : map_) cudaDestroyTextureObject(kv.second);
+    map_.clear();
+  }
+
+ private:
+  typedef std::tuple<uintptr_t, int, int, size_t, int, bool> Key;
+  std::map<Key, cudaTextureObject_t> map_;
+};
+
+}  // namespace vfs

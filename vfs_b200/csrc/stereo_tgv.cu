@@ -1,0 +1,333 @@
+// StereoTgvImpl: device state and the coarse-to-fine schedule of the reference
+// solver (stereotgv/stereotgv.cu:44-598), on one CUDA stream.
+#include <cmath>
+#include <cstring>
+
+#include "stereo_tgv.cuh"
+
+namespace vfs {
+
+StereoTgvImpl::StereoTgvImpl(int bw, int bh, int sa) : blockWidth(bw), blockHeight(bh), strideAlignment(sa) {}
+
+StereoTgvImpl::~StereoTgvImpl() { release(); }
+
+void StereoTgvImpl::release() {
+  tex.clear();
+  if (pool_) cudaFree(pool_);
+  pool_ = nullptr;
+  pool_bytes_ = pool_used_ = 0;
+  initialized_ = false;
+}
+
+float* StereoTgvImpl::alloc(size_t bytes) {
+  size_t off = (pool_used_ + 511) & ~(size_t)511;  // texture base alignment
+  if (off + bytes > pool_bytes_) throw ArgError{"internal: device pool overflow"};
+  pool_used_ = off + bytes;
+  return (float*)(pool_ + off);
+}
+
+static int align_up(int n, int m) {
+  int mod = n % m;
+  return mod ? n + m - mod : n;
+}
+
+// stereotgv.cu:44-168
+void StereoTgvImpl::initialize(const SolverParams& p) {
+  if (p.width <= 0 || p.height <= 0 || p.nLevels <= 0 || p.nWarpIters < 0 || p.nSolverIters < 0 ||
+      !(p.fScale > 0.0f))
+    throw ArgError{"initialize: invalid size or iteration count"};
+  if (strideAlignment <= 0 || blockWidth <= 0 || blockHeight <= 0)
+    throw ArgError{"initialize: invalid block or stride alignment"};
+  release();
+  P = p;
+  width = p.width;
+  height = p.height;
+  stride = align_up(width, strideAlignment);
+  int pitchAlign = 0;
+  int dev = 0;
+  VFS_CUDA(cudaGetDevice(&dev));
+  VFS_CUDA(cudaDeviceGetAttribute(&pitchAlign, cudaDevAttrTexturePitchAlignment, dev));
+  pW.assign(p.nLevels, 0);
+  pH.assign(p.nLevels, 0);
+  pS.assign(p.nLevels, 0);
+  int nh = height, nw = width, ns = stride;
+  for (int l = 0; l < p.nLevels; l++) {
+    if (nw <= 0 || nh <= 0) throw ArgError{"initialize: pyramid level " + std::to_string(l) + " has zero size"};
+    if (((size_t)ns * sizeof(float)) % (size_t)pitchAlign != 0)
+      throw ArgError{"initialize: row pitch is not a multiple of the texture pitch alignment"};
+    pW[l] = nw;
+    pH[l] = nh;
+    pS[l] = ns;
+    nh = (int)((float)nh / p.fScale);
+    nw = (int)((float)nw / p.fScale);
+    ns = align_up(nw, strideAlignment);
+  }
+  full_ = (size_t)stride * height;
+  size_t f = full_ * sizeof(float);
+  // pool: pyramid (5 planes/level: I0, I1, mask, tv x2); full-resolution planes:
+  // 18 float, 10 float2, 1 float4, 2 float3, 1 four-plane staging; u8 and uchar3
+  // image staging; 512 B alignment slack per buffer.
+  size_t bytes = 0;
+  for (int l = 0; l < p.nLevels; l++) bytes += (size_t)pS[l] * pH[l] * sizeof(float) * 5 + 4 * 512;
+  const size_t planes = 18 + 10 * 2 + 4 + 2 * 3 + 4;
+  bytes += f * planes + full_ * (2 + 2 * 3) + 64 * 512;
+  pool_bytes_ = bytes;
+  cudaError_t e = cudaMalloc(&pool_, pool_bytes_);
+  if (e != cudaSuccess) {
+    pool_ = nullptr;
+    (void)cudaGetLastError();
+    throw CudaError{e, "cudaMalloc(solver pool)", __FILE__, __LINE__};
+  }
+  pool_used_ = 0;
+  pI0.assign(p.nLevels, nullptr);
+  pI1.assign(p.nLevels, nullptr);
+  pMask.assign(p.nLevels, nullptr);
+  pTvF.assign(p.nLevels, nullptr);
+  for (int l = 0; l < p.nLevels; l++) {
+    size_t n = (size_t)pS[l] * pH[l] * sizeof(float);
+    pI0[l] = alloc(n);
+    pI1[l] = alloc(n);
+    pMask[l] = alloc(n);
+    pTvF[l] = (float2*)alloc(2 * n);
+  }
+  d_i1calibrated = alloc(f);
+  d_i1warp = alloc(f);
+  d_i0smooth = alloc(f);
+  d_Iu = alloc(f);
+  d_Iz = alloc(f);
+  d_u = alloc(f);
+  d_du = alloc(f);
+  d_us = alloc(f);
+  d_a = alloc(f);
+  d_b = alloc(f);
+  d_c = alloc(f);
+  d_etau = alloc(f);
+  d_etav1 = alloc(f);
+  d_etav2 = alloc(f);
+  d_u_ = alloc(f);
+  d_u_last = alloc(f);
+  d_u_s = alloc(f);
+  d_depth = alloc(f);
+  d_warpUV = (float2*)alloc(2 * f);
+  d_dwarpUV = (float2*)alloc(2 * f);
+  d_warpUVs = (float2*)alloc(2 * f);
+  d_tv2 = (float2*)alloc(2 * f);
+  d_cv = (float2*)alloc(2 * f);
+  d_p = (float2*)alloc(2 * f);
+  d_v = (float2*)alloc(2 * f);
+  d_v_ = (float2*)alloc(2 * f);
+  d_v_s = (float2*)alloc(2 * f);
+  d_Tp = (float2*)alloc(2 * f);
+  d_q = (float4*)alloc(4 * f);
+  d_X = (float3*)alloc(3 * f);
+  d_uvrgb = (float3*)alloc(3 * f);
+  d_i08u = (uint8_t*)alloc(full_);
+  d_i18u = (uint8_t*)alloc(full_);
+  d_i08uc3 = (uchar3*)alloc(3 * full_);
+  d_i18uc3 = (uchar3*)alloc(3 * full_);
+  d_pack = alloc(4 * f);
+  // The reference leaves its buffers uninitialised after cudaMalloc; this
+  // implementation starts from all-zero state so that results are deterministic.
+  VFS_CUDA(cudaMemsetAsync(pool_, 0, pool_bytes_, stream_));
+  VFS_CUDA(cudaStreamSynchronize(stream_));
+  initialized_ = true;
+}
+
+// stereotgv.cu:171-199.  The reference also builds a negated copy of the field
+// (pTvBackward) that the solver never reads; it is not kept here.
+void StereoTgvImpl::loadVectorFields(const float* tv, const float* cvf) {
+  if (!initialized_) throw ArgError{"loadVectorFields before initialize"};
+  if (!tv || !cvf) throw ArgError{"loadVectorFields: null field"};
+  size_t row = (size_t)width * sizeof(float2);
+  VFS_CUDA(cudaMemsetAsync(pTvF[0], 0, full_ * sizeof(float2), stream_));
+  VFS_CUDA(cudaMemsetAsync(d_cv, 0, full_ * sizeof(float2), stream_));
+  VFS_CUDA(cudaMemcpy2DAsync(pTvF[0], (size_t)stride * sizeof(float2), tv, row, row, height, cudaMemcpyHostToDevice,
+                             stream_));
+  VFS_CUDA(cudaMemcpy2DAsync(d_cv, (size_t)stride * sizeof(float2), cvf, row, row, height, cudaMemcpyHostToDevice,
+                             stream_));
+  for (int l = 1; l < P.nLevels; l++) launch_downscale(t2(pTvF[l - 1], l - 1), 2, (float*)pTvF[l], geom(l), stream_);
+  VFS_CUDA(cudaStreamSynchronize(stream_));
+}
+
+// stereotgv.cu:241-252
+void StereoTgvImpl::copyMaskToDevice(const float* mask) {
+  if (!initialized_) throw ArgError{"copyMaskToDevice before initialize"};
+  if (!mask) throw ArgError{"copyMaskToDevice: null mask"};
+  size_t row = (size_t)width * sizeof(float);
+  VFS_CUDA(cudaMemsetAsync(pMask[0], 0, full_ * sizeof(float), stream_));
+  VFS_CUDA(cudaMemcpy2DAsync(pMask[0], (size_t)stride * sizeof(float), mask, row, row, height, cudaMemcpyHostToDevice,
+                             stream_));
+  for (int l = 1; l < P.nLevels; l++) launch_downscale_nearest(t1(pMask[l - 1], l - 1, false), pMask[l], geom(l), stream_);
+  VFS_CUDA(cudaStreamSynchronize(stream_));
+}
+
+// stereotgv.cu:201-213 (u8) and 215-239 (f32, u8c3)
+void StereoTgvImpl::copyImagesU8(const uint8_t* i0, const uint8_t* i1, bool device_src) {
+  if (!initialized_) throw ArgError{"copyImagesToDevice before initialize"};
+  if (!i0 || !i1) throw ArgError{"copyImagesToDevice: null image"};
+  cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  VFS_CUDA(cudaMemcpy2DAsync(d_i08u, stride, i0, width, width, height, kind, stream_));
+  VFS_CUDA(cudaMemcpy2DAsync(d_i18u, stride, i1, width, width, height, kind, stream_));
+  launch_cv8u_to_gray(d_i08u, pI0[0], geom(0), stream_);
+  launch_cv8u_to_gray(d_i18u, pI1[0], geom(0), stream_);
+  if (!device_src) VFS_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void StereoTgvImpl::copyImagesF32(const float* i0, const float* i1) {
+  if (!initialized_) throw ArgError{"copyImagesToDevice before initialize"};
+  if (!i0 || !i1) throw ArgError{"copyImagesToDevice: null image"};
+  size_t row = (size_t)width * sizeof(float);
+  VFS_CUDA(cudaMemcpy2DAsync(pI0[0], (size_t)stride * sizeof(float), i0, row, row, height, cudaMemcpyHostToDevice,
+                             stream_));
+  VFS_CUDA(cudaMemcpy2DAsync(pI1[0], (size_t)stride * sizeof(float), i1, row, row, height, cudaMemcpyHostToDevice,
+                             stream_));
+  VFS_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void StereoTgvImpl::copyImagesU8C3(const uint8_t* i0, const uint8_t* i1) {
+  if (!initialized_) throw ArgError{"copyImagesToDevice before initialize"};
+  if (!i0 || !i1) throw ArgError{"copyImagesToDevice: null image"};
+  size_t row = (size_t)width * 3;
+  VFS_CUDA(cudaMemcpy2DAsync(d_i08uc3, (size_t)stride * 3, i0, row, row, height, cudaMemcpyHostToDevice, stream_));
+  VFS_CUDA(cudaMemcpy2DAsync(d_i18uc3, (size_t)stride * 3, i1, row, row, height, cudaMemcpyHostToDevice, stream_));
+  launch_cv8uc3_to_gray(d_i08uc3, pI0[0], geom(0), stream_);
+  launch_cv8uc3_to_gray(d_i18uc3, pI1[0], geom(0), stream_);
+  VFS_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void StereoTgvImpl::solve(bool masked) {
+  if (!initialized_) throw ArgError{"solve before initialize"};
+  solveReference(masked);
+}
+
+// stereotgv.cu:389-515 (masked) and 256-387 (plain).  Pointer swaps are the
+// reference's Swap() calls; the plain form skips the median filter like the
+// reference (stereotgv.cu:350-351 is commented out).
+void StereoTgvImpl::solveReference(bool masked) {
+  cudaStream_t st = stream_;
+  const size_t f = full_ * sizeof(float);
+  launch_warp_image(t1(pI1[0], 0), d_cv, d_i1calibrated, geom(0), st);
+  std::swap(pI1[0], d_i1calibrated);
+  VFS_CUDA(cudaMemsetAsync(d_u, 0, f, st));
+  VFS_CUDA(cudaMemsetAsync(d_u_, 0, f, st));
+  VFS_CUDA(cudaMemsetAsync(d_warpUV, 0, 2 * f, st));
+  for (int l = 1; l < P.nLevels; l++) {
+    launch_downscale(t1(pI0[l - 1], l - 1), 1, pI0[l], geom(l), st);
+    launch_downscale(t1(pI1[l - 1], l - 1), 1, pI1[l], geom(l), st);
+  }
+  for (int level = P.nLevels - 1; level >= 0; level--) {
+    Geom g = geom(level);
+    const float* mk = masked ? pMask[level] : nullptr;
+    for (float* b : {d_a, d_b, d_c, d_etau, d_etav1, d_etav2, d_i0smooth}) VFS_CUDA(cudaMemsetAsync(b, 0, f, st));
+    const float eta_p = 3.0f, eta_q = 2.0f;
+    if (level == P.nLevels - 1) launch_optical_flow_vector(d_u, pTvF[level], d_warpUV, g, st);
+    launch_gaussian(t1(pI0[level], level), mk, d_i0smooth, g, st);
+    int xcov = ((g.h + blockWidth - 1) / blockWidth) * blockWidth;  // calcTensor.cu:81,227
+    launch_calc_tensor(t1(d_i0smooth, level), mk, P.beta, P.gamma, d_a, d_b, d_c, g, std::min(g.w, xcov), st);
+    launch_solve_eta(mk, P.alpha0, P.alpha1, d_a, d_b, d_c, d_etau, d_etav1, d_etav2, g, st);
+    for (int warpIter = 0; warpIter < P.nWarpIters; warpIter++) {
+      VFS_CUDA(cudaMemsetAsync(d_p, 0, 2 * f, st));
+      VFS_CUDA(cudaMemsetAsync(d_q, 0, 4 * f, st));
+      VFS_CUDA(cudaMemsetAsync(d_v, 0, 2 * f, st));
+      launch_clone2(d_v_, d_v, g, st);
+      VFS_CUDA(cudaMemsetAsync(d_du, 0, f, st));
+      launch_find_warping_vector(t2(pTvF[level], level), d_warpUV, d_tv2, g, st);
+      launch_warp_image(t1(pI1[level], level), d_warpUV, d_i1warp, g, st);
+      launch_derivatives_fisheye(t1(pI0[level], level), t1(d_i1warp, level), pTvF[level], d_Iu, d_Iz, g, st);
+      launch_clone(d_u_last, d_u, g, st);
+      // host step schedule in float (stereotgv.cu:449-456, 476-477)
+      float tau = 1.0f;
+      float sigma = 1.0f / tau;
+      for (int iter = 0; iter < P.nSolverIters; iter++) {
+        float mu;
+        if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P.timestep_lambda);
+        else mu = 1;
+        DualArgs da{mk, d_u_, d_v_, d_a, d_b, d_c, d_p, d_q, P.alpha0, P.alpha1, sigma, eta_p, eta_q};
+        launch_update_dual(da, g, st);
+        launch_solve_tp(mk, d_a, d_b, d_c, d_p, d_Tp, g, st);
+        ThreshArgs ta{mk, d_Tp, d_u_, d_Iu, d_Iz, d_etau, d_u, d_us, P.lambda, tau};
+        launch_thresholding(ta, g, st);
+        std::swap(d_u, d_us);
+        PrimalArgs pa{mk, d_u_, d_v_, d_p, d_q, d_a, d_b, d_c, d_etav1, d_etav2, d_u, d_v, d_u_s, d_v_s,
+                      tau, P.alpha0, P.alpha1, mu};
+        launch_update_primal(pa, g, st);
+        std::swap(d_u_, d_u_s);
+        std::swap(d_v_, d_v_s);
+        sigma = sigma / mu;
+        tau = tau * mu;
+      }
+      if (masked) {
+        launch_median5(d_u, d_us, g, st);
+        std::swap(d_u, d_us);
+      }
+      launch_warp_epilogue(d_u, d_u_last, d_du, d_u_, d_tv2, d_dwarpUV, d_warpUV, P.limitRange, g, st);
+    }
+    if (level > 0) {
+      Geom gf = geom(level - 1);
+      float scale = P.fScale;
+      launch_upscale(t1(d_u, level), 1, d_us, scale, gf, st);
+      launch_upscale(t1(d_u_, level), 1, d_u_s, scale, gf, st);
+      launch_upscale(t2(d_warpUV, level), 2, (float*)d_warpUVs, scale, gf, st);
+      std::swap(d_u, d_us);
+      std::swap(d_u_, d_u_s);
+      std::swap(d_warpUV, d_warpUVs);
+    }
+  }
+}
+
+// stereotgv.cu:517-568 outputs: level-0 views of u, warpUV, the warped image.
+void StereoTgvImpl::copyOut(const char* what, float* dst, bool to_host) {
+  if (!initialized_) throw ArgError{"copy before initialize"};
+  if (!dst) throw ArgError{"copy: null destination"};
+  const void* src = nullptr;
+  int comps = 1;
+  if (!std::strcmp(what, "u")) src = d_u;
+  else if (!std::strcmp(what, "warpUV")) { src = d_warpUV; comps = 2; }
+  else if (!std::strcmp(what, "i1warp")) src = d_i1warp;
+  else if (!std::strcmp(what, "depth")) src = d_depth;
+  else if (!std::strcmp(what, "X")) { src = d_X; comps = 3; }
+  else if (!std::strcmp(what, "rgb")) { src = d_uvrgb; comps = 3; }
+  else throw ArgError{std::string("copy: unknown buffer ") + what};
+  size_t row = (size_t)width * comps * sizeof(float);
+  VFS_CUDA(cudaMemcpy2DAsync(dst, row, src, (size_t)stride * comps * sizeof(float), row, height,
+                             to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, stream_));
+  if (to_host) VFS_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void StereoTgvImpl::convertKB(float fx, float fy, float cx, float cy, float d1, float d2, float d3, float d4, float t1_,
+                              float t2_, float t3_) {
+  if (!initialized_) throw ArgError{"copyStereoToHost before initialize"};
+  launch_convert_kb(d_warpUV, fx, fy, cx, cy, d1, d2, d3, d4, t1_, t2_, t3_, d_X, d_depth, geom(0), stream_);
+}
+
+void StereoTgvImpl::flowToHSV(float flowscale) {
+  if (!initialized_) throw ArgError{"copyDisparityVisToHost before initialize"};
+  launch_flow_to_hsv(d_warpUV, d_uvrgb, flowscale, geom(0), stream_);
+}
+
+void StereoTgvImpl::debugGet(const char* name, int comps, float* out) {
+  if (!initialized_) throw ArgError{"debug get before initialize"};
+  struct E {
+    const char* n;
+    const void* p;
+    int c;
+  } tab[] = {{"u", d_u, 1},          {"u_", d_u_, 1},         {"warpUV", d_warpUV, 2}, {"a", d_a, 1},
+             {"b", d_b, 1},          {"c", d_c, 1},           {"etau", d_etau, 1},     {"etav1", d_etav1, 1},
+             {"etav2", d_etav2, 1},  {"Iu", d_Iu, 1},         {"Iz", d_Iz, 1},         {"i1warp", d_i1warp, 1},
+             {"tv2", d_tv2, 2},      {"i0smooth", d_i0smooth, 1}, {"p", d_p, 2},       {"q", d_q, 4},
+             {"v_", d_v_, 2},        {"Tp", d_Tp, 2},         {"us", d_us, 1},         {"u_s", d_u_s, 1},
+             {"v_s", d_v_s, 2},      {"du", d_du, 1},         {"u_last", d_u_last, 1}, {"X", d_X, 3},
+             {"depth", d_depth, 1},  {"warpUVs", d_warpUVs, 2}, {"i1calibrated", d_i1calibrated, 1}};
+  for (auto& e : tab) {
+    if (std::strcmp(e.n, name)) continue;
+    if (comps != e.c) throw ArgError{"debug get: component count mismatch"};
+    size_t row = (size_t)width * comps * sizeof(float);
+    VFS_CUDA(cudaMemcpy2DAsync(out, row, e.p, (size_t)stride * comps * sizeof(float), row, height,
+                               cudaMemcpyDeviceToHost, stream_));
+    VFS_CUDA(cudaStreamSynchronize(stream_));
+    return;
+  }
+  throw ArgError{std::string("debug get: unknown buffer ") + name};
+}
+
+}  // namespace vfs

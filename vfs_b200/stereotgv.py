@@ -1,0 +1,188 @@
+"""Python mirror of the reference ``StereoTgv`` class (stereotgv/stereotgv.h:14-124).
+
+Method names, argument order and meaning follow the reference; ``cv::Mat`` arguments become
+numpy arrays (H x W, H x W x 2 or H x W x 3) and ``cv::Mat&`` outputs become return values.
+Device-resident inputs and outputs are also accepted as torch CUDA tensors through the
+``*_device`` methods.  All work runs in the CUDA library (vfs_b200/_lib); failures raise
+:class:`VfsError` with the library's status and message.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Tuple
+
+import numpy as np
+
+from ._native import VfsError, check, lib
+
+__all__ = ["StereoTgv", "VfsError"]
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class StereoTgv:
+    """Variational fisheye stereo solver on one GPU (one camera pair)."""
+
+    def __init__(self, blockWidth: int = 32, blockHeight: int = 1, strideAlignment: int = 32):
+        self._L = lib()
+        h = ctypes.c_void_p()
+        st = self._L.vfs_create_ex(ctypes.byref(h), blockWidth, blockHeight, strideAlignment)
+        if st != 0:
+            raise VfsError(st, (self._L.vfs_last_error(None) or b"").decode())
+        self._h = h
+        self.BlockWidth, self.BlockHeight, self.StrideAlignment = blockWidth, blockHeight, strideAlignment
+        self._limit_range = 1.0  # stereotgv.h:45
+        self.baseline = 0.0
+        self.focal = 0.0
+        self.width = self.height = 0
+        self._stream = None
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                self._L.vfs_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- configuration ---------------------------------------------------
+    @property
+    def limitRange(self) -> float:
+        return self._limit_range
+
+    @limitRange.setter
+    def limitRange(self, v: float) -> None:
+        self._limit_range = float(v)
+        check(self._h, self._L.vfs_set_limit_range(self._h, self._limit_range))
+
+    def set_stream(self, stream) -> None:
+        """Run on a torch.cuda.Stream (or a raw cudaStream_t integer)."""
+        raw = getattr(stream, "cuda_stream", stream)
+        self._stream = stream
+        check(self._h, self._L.vfs_set_stream(self._h, ctypes.c_void_p(int(raw) if raw else 0)))
+
+    def synchronize(self) -> None:
+        check(self._h, self._L.vfs_synchronize(self._h))
+
+    # ---- reference methods -------------------------------------------------
+    def initialize(self, width, height, beta, gamma, alpha0, alpha1, timestep_lambda, lambda_,
+                   nLevels, fScale, nWarpIters, nSolverIters) -> int:
+        check(self._h, self._L.vfs_initialize(self._h, int(width), int(height), beta, gamma, alpha0, alpha1,
+                                              timestep_lambda, lambda_, int(nLevels), fScale, int(nWarpIters),
+                                              int(nSolverIters)))
+        self.width, self.height = int(width), int(height)
+        check(self._h, self._L.vfs_set_camera(self._h, float(self.baseline), float(self.focal)))
+        return 0
+
+    def level_sizes(self):
+        out = []
+        w, h, s = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        lvl = 0
+        while True:
+            st = self._L.vfs_get_level_size(self._h, lvl, ctypes.byref(w), ctypes.byref(h), ctypes.byref(s))
+            if st != 0:
+                break
+            out.append((w.value, h.value, s.value))
+            lvl += 1
+        return out
+
+    def loadVectorFields(self, translationVector: np.ndarray, calibrationVector: np.ndarray) -> int:
+        tv = np.ascontiguousarray(translationVector, np.float32)
+        cv = np.ascontiguousarray(calibrationVector, np.float32)
+        self._check_shape(tv, (self.height, self.width, 2), "translationVector")
+        self._check_shape(cv, (self.height, self.width, 2), "calibrationVector")
+        check(self._h, self._L.vfs_load_vector_fields(self._h, _ptr(tv), _ptr(cv)))
+        return 0
+
+    def copyMaskToDevice(self, mask: np.ndarray) -> int:
+        m = np.ascontiguousarray(mask, np.float32)
+        self._check_shape(m, (self.height, self.width), "mask")
+        check(self._h, self._L.vfs_copy_mask_to_device(self._h, _ptr(m)))
+        return 0
+
+    def copyImagesToDevice(self, i0, i1) -> int:
+        """u8 (H x W), float32 (H x W) or u8 colour (H x W x 3) images, as the reference overloads."""
+        a = np.asarray(i0)
+        b = np.asarray(i1)
+        if a.dtype != b.dtype or a.shape != b.shape:
+            raise VfsError(-1, "copyImagesToDevice: images differ in type or shape")
+        if a.dtype == np.uint8 and a.ndim == 2:
+            self._check_shape(a, (self.height, self.width), "image")
+            a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+            check(self._h, self._L.vfs_copy_images_to_device_u8(self._h, _ptr(a), _ptr(b)))
+        elif a.dtype == np.uint8 and a.ndim == 3 and a.shape[2] == 3:
+            self._check_shape(a, (self.height, self.width, 3), "image")
+            a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+            check(self._h, self._L.vfs_copy_images_to_device_u8c3(self._h, _ptr(a), _ptr(b)))
+        elif a.dtype == np.float32 and a.ndim == 2:
+            self._check_shape(a, (self.height, self.width), "image")
+            a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+            check(self._h, self._L.vfs_copy_images_to_device_f32(self._h, _ptr(a), _ptr(b)))
+        else:
+            raise VfsError(-1, f"copyImagesToDevice: unsupported image type {a.dtype} {a.shape}")
+        return 0
+
+    def copy_images_from_device(self, d_i0, d_i1) -> None:
+        """Images already on the GPU: tight H x W uint8 torch tensors (stream-ordered)."""
+        for t in (d_i0, d_i1):
+            if not (t.is_cuda and t.is_contiguous() and tuple(t.shape) == (self.height, self.width)):
+                raise VfsError(-1, "copy_images_from_device: need contiguous H x W uint8 CUDA tensors")
+        check(self._h, self._L.vfs_copy_images_from_device_u8(self._h, ctypes.c_void_p(d_i0.data_ptr()),
+                                                              ctypes.c_void_p(d_i1.data_ptr())))
+
+    def solveStereoForward(self) -> int:
+        check(self._h, self._L.vfs_solve_stereo_forward(self._h))
+        return 0
+
+    def solveStereoForwardMasked(self) -> int:
+        check(self._h, self._L.vfs_solve_stereo_forward_masked(self._h))
+        return 0
+
+    def copy1DDisparityToHost(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        check(self._h, self._L.vfs_copy_1d_disparity_to_host(self._h, _ptr(out)))
+        return out
+
+    def copyDisparityToHost(self) -> np.ndarray:
+        out = np.empty((self.height, self.width, 2), np.float32)
+        check(self._h, self._L.vfs_copy_disparity_to_host(self._h, _ptr(out)))
+        return out
+
+    def copyWarpedImageToHost(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        check(self._h, self._L.vfs_copy_warped_image_to_host(self._h, _ptr(out)))
+        return out
+
+    def copy_1d_disparity_to_device(self, d_out) -> None:
+        if not (d_out.is_cuda and d_out.is_contiguous() and tuple(d_out.shape) == (self.height, self.width)):
+            raise VfsError(-1, "copy_1d_disparity_to_device: need a contiguous H x W float32 CUDA tensor")
+        check(self._h, self._L.vfs_copy_1d_disparity_to_device(self._h, ctypes.c_void_p(d_out.data_ptr())))
+
+    def copyStereoToHost(self, focalx, focaly, cx, cy, d1, d2, d3, d4, t1, t2, t3) -> Tuple[np.ndarray, np.ndarray]:
+        depth = np.empty((self.height, self.width), np.float32)
+        X = np.empty((self.height, self.width, 3), np.float32)
+        check(self._h, self._L.vfs_copy_stereo_to_host(self._h, _ptr(depth), _ptr(X), focalx, focaly, cx, cy,
+                                                       d1, d2, d3, d4, t1, t2, t3))
+        return depth, X
+
+    def copyDisparityVisToHost(self, flowScale: float) -> np.ndarray:
+        out = np.empty((self.height, self.width, 3), np.float32)
+        check(self._h, self._L.vfs_copy_disparity_vis_to_host(self._h, _ptr(out), flowScale))
+        return out
+
+    def debug_buffer(self, name: str, comps: int = 1) -> np.ndarray:
+        out = np.empty((self.height, self.width, comps), np.float32)
+        check(self._h, self._L.vfs_debug_get_buffer(self._h, name.encode(), comps, _ptr(out)))
+        return out[:, :, 0] if comps == 1 else out
+
+    @staticmethod
+    def _check_shape(a: np.ndarray, shape, what: str) -> None:
+        if tuple(a.shape) != tuple(shape):
+            raise VfsError(-1, f"{what}: expected shape {tuple(shape)}, got {tuple(a.shape)}")
