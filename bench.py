@@ -1,0 +1,460 @@
+#!/usr/bin/env python
+"""Benchmark of the variational fisheye stereo solve on B200.
+
+One *step* is one solve of every pair in the rank's batch of seeded synthetic 848x800
+fisheye pairs (5 pyramid levels x 3 warps x 50 primal-dual iterations, masked solve, the
+reference's solver settings).  ``value`` is whole-job frames/s with inputs resident in HBM;
+``e2e`` is the same metric through the public API with pinned host buffers (H2D of both
+images and D2H of the disparity inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--path fused|plain] [--batch B]
+    python bench.py --impl reference ...   # the CPU restatement of the reference on host cores
+
+Under torchrun every rank runs its own replica (the solve has no cross-GPU exchange); the
+job value is all frames over the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "848×800 stereo frames/s + p99 latency, fused vs plain, at ≤0.05px mean err"
+W0, H0 = 848, 800
+B_ALG_FP32 = 116.0  # algorithmic bytes per pixel-iteration of the inner loop, FP32 storage
+B_ALG_FP16 = 84.0   # with p, q, v in FP16
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--path", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--batch", type=int, default=0, help="pairs per rank (default: 8 fused, 1 plain)")
+    ap.add_argument("--storage", default="fp16", choices=["fp16", "fp32"], help="fused path: p, q, v-bar storage")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in comparison run")
+    ap.add_argument("--seed", type=int, default=20260)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def pair_cache(w, h, seed):
+    """Synthetic pair, cached under /tmp so repeated runs on one machine skip rendering."""
+    from vfs_b200 import synth
+    path = f"/tmp/vfs_b200_pair_{w}x{h}_{seed}.npz"
+    if os.path.exists(path):
+        try:
+            d = np.load(path)
+            return dict(i0=d["i0"], i1=d["i1"], mask=d["mask"], tv=d["tv"], cv=d["cv"])
+        except Exception:
+            pass
+    p = synth.make_pair(w, h, seed)
+    d = dict(i0=p.i0, i1=p.i1, mask=p.mask, tv=p.tv, cv=p.cv)
+    try:
+        np.savez(path, **d)
+    except OSError:
+        pass
+    return d
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    for p in (os.path.join(ROOT, "MEASURED_PEAKS.json"),):
+        try:
+            d = json.load(open(p))
+            return float(d["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    try:
+        d = json.load(open(p))
+        return d.get(kernel_key)
+    except Exception:
+        return None
+
+
+def make_solver(pair, path, stream, half=False):
+    from vfs_b200 import synth
+    from vfs_b200.stereotgv import StereoTgv
+    sp = synth.SOLVER_PARAMS
+    s = StereoTgv()
+    s.set_solve_path(path == "fused", half)
+    s.limitRange = synth.LIMIT_RANGE
+    s.initialize(W0, H0, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"], sp["lambda_"],
+                 synth.n_levels_for(W0), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+    s.copyMaskToDevice(pair["mask"])
+    s.loadVectorFields(pair["tv"], pair["cv"])
+    s.set_stream(stream)
+    return s
+
+
+def cpu_baseline(pair, budget_s=12.0, precision=64):
+    """Time the CPU oracle (all host threads) on the workload; returns (frames/s, threads, u of the last frame)."""
+    from oracle.oracle import OracleStereoTgv
+    from vfs_b200 import synth
+    sp = synth.SOLVER_PARAMS
+    o = OracleStereoTgv(precision)
+    o.set_limit_range(synth.LIMIT_RANGE)
+    o.initialize(W0, H0, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"], sp["lambda_"],
+                 synth.n_levels_for(W0), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+    o.copy_mask_to_device(pair["mask"])
+    o.load_vector_fields(pair["tv"], pair["cv"])
+    n, t0 = 0, time.perf_counter()
+    while True:
+        o.copy_images_to_device(pair["i0"], pair["i1"])
+        o.solve_stereo_forward_masked()
+        n += 1
+        if time.perf_counter() - t0 >= budget_s:
+            break
+    dt = time.perf_counter() - t0
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    return n / dt, threads, o.get("u"), n, dt
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's solver restated on the host (the reference has no CPU
+    path of its own and its CUDA build cannot be compiled here), all host threads."""
+    if rank != 0:
+        return
+    pair = pair_cache(W0, H0, args.seed)
+    from oracle.oracle import OracleStereoTgv, build as build_oracle
+    from vfs_b200 import synth
+    build_oracle()
+    sp = synth.SOLVER_PARAMS
+    o = OracleStereoTgv(32)
+    o.set_limit_range(synth.LIMIT_RANGE)
+    o.initialize(W0, H0, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"], sp["lambda_"],
+                 synth.n_levels_for(W0), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+    o.copy_mask_to_device(pair["mask"])
+    o.load_vector_fields(pair["tv"], pair["cv"])
+
+    def step():
+        o.copy_images_to_device(pair["i0"], pair["i1"])
+        o.solve_stereo_forward_masked()
+
+    t0 = time.perf_counter()
+    step()
+    t_frame = time.perf_counter() - t0
+    budget = 150.0
+    warm = max(0, min(args.warmup - 1, int(budget * 0.2 / max(t_frame, 1e-3))))
+    steps = max(1, min(args.steps, int(budget * 0.8 / max(t_frame, 1e-3))))
+    for _ in range(warm):
+        step()
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        step()
+        times.append(time.perf_counter() - t)
+    tot = sum(times)
+    fps = steps / tot
+    threads = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": fps, "unit": "frames/s", "n_gpus": world, "steps": steps,
+        "warmup": warm + 1, "ms_per_step": 1000 * tot / steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "848x800 fisheye stereo pair, masked TGV-L1 solve, 5 levels x 3 warps x 50 iterations",
+                   "batch": 1, "seed": args.seed},
+        "latency_ms": {"p50": 1000 * float(np.percentile(times, 50)), "p99": 1000 * float(np.percentile(times, 99))},
+        "cpu_baseline": {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} full 848x800 frames, float32 restatement of the reference solver, "
+                                   f"OpenMP over rows"},
+        "e2e": {"value": fps, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def plain_reference_run(pair, dev, flush, steps=6):
+    """The drop-in path (one kernel per reference kernel, FP32, one pair at a time) on the
+    same GPU and inputs: frames/s with device-resident inputs, L2 flushed before each frame."""
+    import torch
+    st = torch.cuda.Stream(device=dev)
+    s = make_solver(pair, "plain", st)
+    a = torch.from_numpy(pair["i0"]).to(dev)
+    b = torch.from_numpy(pair["i1"]).to(dev)
+    for _ in range(2):
+        s.copy_images_from_device(a, b)
+        s.solveStereoForwardMasked()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        with torch.cuda.stream(st):
+            flush.fill_(3.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        s.copy_images_from_device(a, b)
+        s.solveStereoForwardMasked()
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return {"value": 1000.0 / float(np.mean(ms)), "unit": "frames/s", "ms_per_frame": float(np.mean(ms)),
+            "p99_ms": float(np.percentile(ms, 99)), "storage": "fp32", "batch": 1}
+
+
+def run_ours(args, rank, world, local):
+    import torch
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    from vfs_b200.build import build
+    if rank == 0:
+        build()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist.barrier()
+        build()  # other ranks see the built library (no-op when current)
+    from vfs_b200.stereotgv import StereoBatch, StereoTgv
+    fused = args.path == "fused"
+    half = fused and args.storage == "fp16"
+    batch = args.batch or (8 if fused else 1)
+    pairs = [pair_cache(W0, H0, args.seed + 1000 * rank + k) for k in range(batch)]
+    stream = torch.cuda.Stream(device=dev)
+    solvers = [make_solver(p, args.path, stream, half) for p in pairs]
+    sbatch = None
+    if fused:
+        sbatch = StereoBatch(half_storage=half, stream=stream)
+        for s in solvers:
+            sbatch.add(s)
+    d_imgs = [(torch.from_numpy(p["i0"]).to(dev), torch.from_numpy(p["i1"]).to(dev)) for p in pairs]
+    d_out = [torch.empty((H0, W0), dtype=torch.float32, device=dev) for _ in pairs]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # 256 MiB > L2
+    torch.cuda.synchronize()
+
+    def device_step():
+        if fused:
+            for s, (a, b) in zip(solvers, d_imgs):
+                s.copy_images_from_device(a, b)
+            sbatch.solve(True)
+            for s, o in zip(solvers, d_out):
+                s.copy_1d_disparity_to_device(o)
+            return
+        for s, (a, b), o in zip(solvers, d_imgs, d_out):
+            s.copy_images_from_device(a, b)
+            s.solveStereoForwardMasked()
+            s.copy_1d_disparity_to_device(o)
+
+    for _ in range(args.warmup):
+        device_step()
+        flush.fill_(1.0)
+    torch.cuda.synchronize()
+
+    # ---- timed region: device-resident inputs -----------------------------------------
+    for s in solvers:
+        s.profile(True)
+        s.profile_reset()
+    launches0 = StereoTgv.launch_count()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(float(k))  # evict the previous step's working set from L2
+            ev[k][0].record(stream)
+            device_step()
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches = StereoTgv.launch_count() - launches0
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    total_ms = float(sum(step_ms))
+    # roofline of the inner primal-dual loop: kind 0 (drop-in, one record per iteration)
+    kind = 1 if args.path == "fused" else 0
+    n_l = ms_l = pi_l = 0.0
+    for s in solvers:
+        n, ms, pi = s.profile_read(kind)
+        n_l += n
+        ms_l += ms
+        pi_l += pi
+        s.profile(False)
+    if world > 1:
+        t = torch.tensor([total_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    frames = batch * args.steps * world
+    value = frames / (total_ms / 1000.0)
+
+    # ---- e2e: the public API with pinned host buffers -----------------------------------
+    h_in = []
+    for p in pairs:
+        a = torch.from_numpy(p["i0"]).pin_memory().numpy()
+        b = torch.from_numpy(p["i1"]).pin_memory().numpy()
+        h_in.append((a, b))
+    for s in solvers:
+        s.set_stream(stream)
+    e2e_steps = max(3, min(args.steps, 10))
+
+    def host_step():
+        outs = []
+        if fused:
+            for s, (a, b) in zip(solvers, h_in):
+                s.copyImagesToDevice(a, b)
+            sbatch.solve(True)
+            return [s.copy1DDisparityToHost() for s in solvers]
+        for s, (a, b) in zip(solvers, h_in):
+            s.copyImagesToDevice(a, b)
+            s.solveStereoForwardMasked()
+            outs.append(s.copy1DDisparityToHost())
+        return outs
+
+    host_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    e2e_ms = []
+    for _ in range(e2e_steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(2.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        outs = host_step()
+        e2e_ms.append(1000 * (time.perf_counter() - t0))
+    e2e_total = float(sum(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_total], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = batch * e2e_steps * world / (e2e_total / 1000.0)
+    gpu_u = outs[0]
+
+    result = None
+    if rank == 0:
+        peak, peak_kind = measured_peak()
+        b_alg = B_ALG_FP16 if half else B_ALG_FP32
+        achieved = (pi_l * b_alg / (ms_l / 1000.0) / 1e9) if ms_l > 0 else None
+        kernel_key = "fused_inner" if args.path == "fused" else "plain_inner_iteration"
+        tr = ncu_traffic(kernel_key)
+        traffic = None
+        if tr and n_l > 0:
+            traffic = tr.get("dram_bytes_per_pixel_iteration", 0) * pi_l / n_l
+        per_frame = np.array(step_ms) / (1 if fused else batch)
+        result = {
+            "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "848x800 fisheye stereo pairs, masked TGV-L1 solve, 5 levels x 3 warps x 50 iterations",
+                       "path": args.path, "batch_per_gpu": batch, "storage": "fp16" if half else "fp32",
+                       "l2": "flushed (256 MiB write) before every step",
+                       "seed": args.seed, "parallelism": f"replicas x{world}"},
+            "latency_ms": {"p50": float(np.percentile(per_frame, 50)), "p99": float(np.percentile(per_frame, 99)),
+                           "note": "per frame; a batched step completes all its frames together"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                         "kernel": kernel_key, "launches_timed": int(n_l),
+                         "bytes_per_pixel_iteration": b_alg, "peak_kind": peak_kind},
+            "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": batch * 2 * W0 * H0,
+                    "d2h_bytes_per_step": batch * W0 * H0 * 4},
+            "gpu_launches": int(launches),
+            "clocks": clocks.summary(),
+        }
+        if fused and not args.no_plain:
+            result["plain_dropin"] = plain_reference_run(pairs[0], dev, flush)
+            result["speedup_vs_plain"] = value / result["plain_dropin"]["value"] / world
+        if world == 1 and not args.no_cpu_baseline:
+            fps, threads, u_cpu, n, dt = cpu_baseline(pairs[0])
+            m = pairs[0]["mask"] > 0
+            d = np.abs(gpu_u.astype(np.float64) - u_cpu)[m]
+            result["cpu_baseline"] = {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
+                                      "sample": f"{n} full 848x800 frame(s) in {dt:.1f} s, float64 oracle "
+                                                f"(CPU restatement of the reference solver), OpenMP over rows"}
+            result["accuracy_vs_fp64_oracle"] = {"mean_abs_px": float(d.mean()), "max_abs_px": float(d.max()),
+                                                 "bad_1px_rate": float((d > 1.0).mean())}
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return result
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

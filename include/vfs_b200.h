@@ -103,6 +103,48 @@ int vfs_copy_disparity_vis_to_host(vfs_stereo* s, float* rgb, float flow_scale);
  * "tv2", "p", "q", "Tp", ...) to host memory. */
 int vfs_debug_get_buffer(vfs_stereo* s, const char* name, int comps, float* out);
 
+/* ---- fast path (no counterpart in the reference) ---------------------------------
+ * vfs_set_solve_path selects how vfs_solve_stereo_forward[_masked] runs:
+ *   VFS_PATH_REFERENCE: one kernel per reference kernel, in the reference's order;
+ *   VFS_PATH_FUSED: one fused kernel per primal-dual iteration plus fused per-warp and
+ *   per-level kernels, replayed as a CUDA graph.  With float storage the fused path gives
+ *   bit-identical results; with half storage (half_storage = 1) p, q and v-bar are kept
+ *   as IEEE half in memory (all arithmetic stays float). */
+#define VFS_PATH_REFERENCE 0
+#define VFS_PATH_FUSED 1
+int vfs_set_solve_path(vfs_stereo* s, int path, int half_storage);
+int vfs_set_graph(vfs_stereo* s, int use_graph);
+
+/* Batched solves: several handles (pairs, possibly of different sizes) solved together,
+ * one launch per step and pyramid level for all of them, replayed as a CUDA graph.
+ * Pairs of a batch need equal nWarpIters, nSolverIters and timestep_lambda.  The batch
+ * does not own the handles; vfs_batch_add moves the handle onto the batch's stream.  At
+ * most VFS_BATCH_MAX pairs. */
+#define VFS_BATCH_MAX 24
+typedef struct vfs_batch vfs_batch;
+int vfs_batch_create(vfs_batch** out);
+int vfs_batch_destroy(vfs_batch* b);
+const char* vfs_batch_last_error(const vfs_batch* b);
+int vfs_batch_set_stream(vfs_batch* b, void* cuda_stream);
+int vfs_batch_add(vfs_batch* b, vfs_stereo* s);
+int vfs_batch_clear(vfs_batch* b);
+int vfs_batch_size(const vfs_batch* b);
+int vfs_batch_set_storage(vfs_batch* b, int half_storage);
+int vfs_batch_set_graph(vfs_batch* b, int use_graph);
+int vfs_batch_solve(vfs_batch* b, int masked);
+
+/* Measurement hooks (no counterpart in the reference).  vfs_launch_count() is the number
+ * of kernels this library has launched in the process.  With profiling on, each group of
+ * inner primal-dual kernels (one iteration in the drop-in path, one fused launch of several
+ * iterations in the fused path) is bracketed by CUDA events on the handle's stream;
+ * vfs_profile_read() sums the records of a group kind (0 = drop-in inner iteration,
+ * 1 = fused inner launch, 2 = fused per-warp prologue, 3 = fused epilogue). */
+long long vfs_launch_count(void);
+int vfs_profile_enable(vfs_stereo* s, int on);
+int vfs_profile_reset(vfs_stereo* s);
+int vfs_profile_read(vfs_stereo* s, int kind, long long* launches, double* total_ms,
+                     double* pixel_iterations);
+
 /* ---- reference DLL entry points (dllhook/vfs.h:37-44) -------------------------------
  * Create / Init / SolveStereo with the reference's names and argument lists.  Init reads
  * the mask (8-bit PNG or binary PGM, scaled by 1/255) and the two Middlebury .flo fields.

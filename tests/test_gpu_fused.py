@@ -1,0 +1,107 @@
+"""Fused path (one kernel per primal-dual iteration, batched launches, CUDA graphs).
+
+With float storage the fused path performs the drop-in path's operations in the same
+order on the same physical buffers, so the results must be bit-identical, also across
+frames (masked-out pixels keep stale state) and inside batches of uneven sizes.  With half
+storage of p, q and v-bar the bar is the accuracy one: mean |u - u_fp64| <= 0.05 px.
+"""
+import numpy as np
+import pytest
+
+from tests.helpers import diff_stats, params, random_case, run_gpu, run_oracle
+
+pytestmark = pytest.mark.gpu
+
+OUT = (("u", 1), ("u_", 1), ("warpUV", 2), ("i1warp", 1), ("Iu", 1), ("Iz", 1), ("Tp", 2), ("a", 1))
+
+
+def make(i0, i1, mask, tv, cv, p, fused, half=False, graph=True):
+    from vfs_b200.stereotgv import StereoTgv
+    s = StereoTgv()
+    s.set_solve_path(fused, half)
+    s.set_graph(graph)
+    h, w = i0.shape
+    s.limitRange = p["limit_range"]
+    s.initialize(w, h, p["beta"], p["gamma"], p["alpha0"], p["alpha1"], p["tsl"], p["lam"], p["n_levels"],
+                 p["f_scale"], p["n_warp"], p["n_iter"])
+    s.copyMaskToDevice(mask)
+    s.loadVectorFields(tv, cv)
+    return s
+
+
+def solve_frames(s, i0, i1, masked, frames):
+    for _ in range(frames):
+        s.copyImagesToDevice(i0, i1)
+        (s.solveStereoForwardMasked if masked else s.solveStereoForward)()
+    s.synchronize()
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("masked", [True, False])
+@pytest.mark.parametrize("size", [(67, 53), (130, 101)])
+def test_fused_bit_identical_to_dropin(gpu, graph, masked, size):
+    w, h = size
+    i0, i1, mask, tv, cv = random_case(w, h, seed=w + 3 * h)
+    p = params(n_levels=2, n_warp=2, n_iter=7)
+    a = make(i0, i1, mask, tv, cv, p, fused=False)
+    b = make(i0, i1, mask, tv, cv, p, fused=True, graph=graph)
+    for frame in range(3):
+        solve_frames(a, i0, i1, masked, 1)
+        solve_frames(b, i0, i1, masked, 1)
+        for name, comps in OUT:
+            x, y = a.debug_buffer(name, comps), b.debug_buffer(name, comps)
+            assert np.array_equal(x, y), (frame, name, diff_stats(x, y))
+
+
+def test_fused_odd_iteration_count(gpu):
+    # an odd number of inner iterations leaves u in the other ping-pong buffer
+    i0, i1, mask, tv, cv = random_case(90, 70, seed=4)
+    p = params(n_levels=3, n_warp=3, n_iter=5)
+    a = make(i0, i1, mask, tv, cv, p, fused=False)
+    b = make(i0, i1, mask, tv, cv, p, fused=True)
+    solve_frames(a, i0, i1, True, 2)
+    solve_frames(b, i0, i1, True, 2)
+    for name, comps in OUT:
+        assert np.array_equal(a.debug_buffer(name, comps), b.debug_buffer(name, comps)), name
+
+
+def test_batch_uneven_sizes_bit_identical(gpu):
+    from vfs_b200.stereotgv import StereoBatch
+    cases = [(96, 64, 2), (130, 101, 3), (67, 53, 2), (200, 120, 3)]
+    p0 = params(n_warp=2, n_iter=6)
+    singles, members, data = [], [], []
+    batch = StereoBatch()
+    for k, (w, h, L) in enumerate(cases):
+        i0, i1, mask, tv, cv = random_case(w, h, seed=100 + k)
+        p = dict(p0, n_levels=L, alpha0=17.0 + k, limit_range=0.1 + 0.05 * k)
+        data.append((i0, i1))
+        singles.append(make(i0, i1, mask, tv, cv, p, fused=False))
+        m = make(i0, i1, mask, tv, cv, p, fused=True)
+        batch.add(m)
+        members.append(m)
+    for frame in range(2):
+        for s, (i0, i1) in zip(singles, data):
+            solve_frames(s, i0, i1, True, 1)
+        for m, (i0, i1) in zip(members, data):
+            m.copyImagesToDevice(i0, i1)
+        batch.solve(True)
+        for s, m in zip(singles, members):
+            m.synchronize()
+            for name, comps in (("u", 1), ("warpUV", 2)):
+                assert np.array_equal(s.debug_buffer(name, comps), m.debug_buffer(name, comps)), (frame, name)
+
+
+def test_half_storage_accuracy(gpu):
+    from vfs_b200 import synth
+    pair = synth.make_pair(424, 400, seed=77)
+    sp = synth.SOLVER_PARAMS
+    p = params(beta=sp["beta"], gamma=sp["gamma"], n_levels=synth.n_levels_for(424), n_warp=sp["nWarpIters"],
+               n_iter=sp["nSolverIters"], limit_range=synth.LIMIT_RANGE)
+    s = make(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, fused=True, half=True)
+    solve_frames(s, pair.i0, pair.i1, True, 1)
+    u = s.copy1DDisparityToHost()
+    o = run_oracle(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True, precision=64)
+    m = pair.mask > 0
+    d = np.abs(u.astype(np.float64) - o.get("u"))[m]
+    assert d.mean() <= 0.05, d.mean()
+    assert (d > 1.0).mean() < 0.01

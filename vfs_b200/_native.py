@@ -61,14 +61,33 @@ SIGNATURES = {
     "vfs_copy_stereo_to_host": [_vp, _vp, _vp] + [_f] * 11,
     "vfs_copy_disparity_vis_to_host": [_vp, _vp, _f],
     "vfs_debug_get_buffer": [_vp, ctypes.c_char_p, _i, _vp],
+    "vfs_set_solve_path": [_vp, _i, _i],
+    "vfs_set_graph": [_vp, _i],
+    "vfs_batch_create": [ctypes.POINTER(_vp)],
+    "vfs_batch_destroy": [_vp],
+    "vfs_batch_last_error": [_vp],
+    "vfs_batch_set_stream": [_vp, _vp],
+    "vfs_batch_add": [_vp, _vp],
+    "vfs_batch_clear": [_vp],
+    "vfs_batch_size": [_vp],
+    "vfs_batch_set_storage": [_vp, _i],
+    "vfs_batch_set_graph": [_vp, _i],
+    "vfs_batch_solve": [_vp, _i],
+    "vfs_launch_count": [],
+    "vfs_profile_enable": [_vp, _i],
+    "vfs_profile_reset": [_vp],
+    "vfs_profile_read": [_vp, _i, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),
+                         ctypes.POINTER(ctypes.c_double)],
     "Create": [],
     "Init": [_vp, _i, _i, _f, _f, _f, _f, _f, _f, _i, _f, _i, _i, _f, _f, ctypes.c_char_p, ctypes.c_char_p,
              ctypes.c_char_p],
     "SolveStereo": [_vp, _vp, _vp, _vp, _i, _i, _f],
 }
 _RESTYPE = {
+    "vfs_launch_count": ctypes.c_longlong,
     "vfs_status_string": ctypes.c_char_p,
     "vfs_last_error": ctypes.c_char_p,
+    "vfs_batch_last_error": ctypes.c_char_p,
     "Create": _vp,
     "Init": None,
     "SolveStereo": None,
@@ -96,4 +115,10 @@ def lib():
 def check(handle, status: int) -> None:
     if status != VFS_OK:
         msg = lib().vfs_last_error(handle) or b""
+        raise VfsError(status, msg.decode(errors="replace"))
+
+
+def check_batch(handle, status: int) -> None:
+    if status != VFS_OK:
+        msg = lib().vfs_batch_last_error(handle) or b""
         raise VfsError(status, msg.decode(errors="replace"))

@@ -1,0 +1,369 @@
+// Host schedule of the fused path: the reference's coarse-to-fine schedule
+// (stereotgv.cu:389-515 / 256-387) for a batch of pairs, with one batched launch
+// per step and pyramid level, and the reference's pointer swaps applied to every
+// pair.  Pairs may differ in size and pyramid depth; a pair joins the schedule at
+// its own coarsest level.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fused.cuh"
+#include "stereo_tgv.cuh"
+
+namespace vfs {
+
+namespace {
+
+template <class ArgsT>
+void set_tiles(ArgsT& A, int k, int w, int h) {
+  A.pr[k].tiles_x = tiles_x_of(w);
+  A.pr[k].tile0 = A.ntiles;
+  A.ntiles += tiles_of(w, h);
+}
+
+void set_iter_tiles(IterArgs& A, int k, int w, int h) {
+  A.pr[k].tiles_x = iter_tiles_x_of(w);
+  A.pr[k].tile0 = A.ntiles;
+  A.ntiles += iter_tiles_of(w, h);
+}
+
+}  // namespace
+
+void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st) {
+  const int n = (int)pairs.size();
+  if (n == 0) return;
+  if (n > kMaxPairs) throw ArgError{"batch larger than " + std::to_string(kMaxPairs) + " pairs"};
+  const SolverParams& P0 = pairs[0]->P;
+  int maxL = 0;
+  for (auto* s : pairs) {
+    if (!s->initialized()) throw ArgError{"fused solve: pair not initialized"};
+    if (s->P.nWarpIters != P0.nWarpIters || s->P.nSolverIters != P0.nSolverIters ||
+        s->P.timestep_lambda != P0.timestep_lambda)
+      throw ArgError{"fused solve: pairs of one batch need equal warp / iteration counts and timestep_lambda"};
+    s->ensureFused();
+    maxL = std::max(maxL, s->levels());
+  }
+  StereoTgvImpl* prof = pairs[0];
+  // ---- calibration warp, state reset, image pyramid (stereotgv.cu:392-405) ---------
+  for (auto* s : pairs) {
+    launch_warp_image(s->tex1(s->pI1[0], 0), s->d_cv, s->d_i1calibrated, s->geomAt(0), st);
+    std::swap(s->pI1[0], s->d_i1calibrated);
+    size_t f = s->fullElems() * sizeof(float);
+    VFS_CUDA(cudaMemsetAsync(s->d_u, 0, f, st));
+    VFS_CUDA(cudaMemsetAsync(s->d_u_, 0, f, st));
+    VFS_CUDA(cudaMemsetAsync(s->d_warpUV, 0, 2 * f, st));
+  }
+  for (int l = 1; l < maxL; l++) {
+    DownArgs D{};
+    int k = 0;
+    for (auto* s : pairs) {
+      if (l >= s->levels()) continue;
+      DownPair& d = D.pr[k];
+      d.texI0 = s->tex1(s->pI0[l - 1], l - 1);
+      d.texI1 = s->tex1(s->pI1[l - 1], l - 1);
+      d.I0 = s->pI0[l];
+      d.I1 = s->pI1[l];
+      d.w = s->pW[l];
+      d.h = s->pH[l];
+      d.s = s->pS[l];
+      set_tiles(D, k, d.w, d.h);
+      k++;
+    }
+    D.npairs = k;
+    launch_downscale_batched(D, st);
+  }
+  // ---- levels -------------------------------------------------------------------------
+  for (int level = maxL - 1; level >= 0; level--) {
+    std::vector<StereoTgvImpl*> act;
+    for (auto* s : pairs)
+      if (level < s->levels()) act.push_back(s);
+    const int na = (int)act.size();
+    long long px_level = 0;
+    for (auto* s : act) px_level += (long long)s->pW[level] * s->pH[level];
+    {
+      LevelArgs L{};
+      for (int k = 0; k < na; k++) {
+        StereoTgvImpl* s = act[k];
+        LevelPair& d = L.pr[k];
+        d.texI0 = s->tex1(s->pI0[level], level);
+        d.texSmooth = s->tex1(s->d_i0smooth, level);
+        d.mask = masked ? s->pMask[level] : nullptr;
+        d.i0smooth = s->d_i0smooth;
+        d.a = s->d_a;
+        d.b = s->d_b;
+        d.c = s->d_c;
+        d.warpUV = s->d_warpUV;
+        d.u = s->d_u;
+        d.tv = s->pTvF[level];
+        d.init_flow = level == s->levels() - 1;
+        d.w = s->pW[level];
+        d.h = s->pH[level];
+        d.s = s->pS[level];
+        int xcov = ((d.h + s->blockWidth - 1) / s->blockWidth) * s->blockWidth;  // calcTensor.cu:81,227
+        d.xmax = std::min(d.w, xcov);
+        d.beta = s->P.beta;
+        d.gamma = s->P.gamma;
+        set_tiles(L, k, d.w, d.h);
+      }
+      L.npairs = na;
+      launch_level_gaussian(L, st);
+      launch_level_tensor(L, st);
+    }
+    for (int warpIter = 0; warpIter < P0.nWarpIters; warpIter++) {
+      prof->profBeginPx(kProfPrologue, px_level, 1);
+      {
+        WarpStartArgs W{};
+        for (int k = 0; k < na; k++) {
+          StereoTgvImpl* s = act[k];
+          WarpStartPair& d = W.pr[k];
+          d.texI1 = s->tex1(s->pI1[level], level);
+          d.texTv = s->tex2(s->pTvF[level], level);
+          d.warpUV = s->d_warpUV;
+          d.tv2 = s->d_tv2;
+          d.i1warp = s->d_i1warp;
+          d.p = s->f_p;
+          d.q = s->f_q;
+          d.v_ = half ? s->f_vh : (void*)s->d_v_;
+          d.w = s->pW[level];
+          d.h = s->pH[level];
+          d.s = s->pS[level];
+          set_tiles(W, k, d.w, d.h);
+        }
+        W.npairs = na;
+        launch_warp_start(W, half, st);
+      }
+      {
+        DerivArgs Dv{};
+        for (int k = 0; k < na; k++) {
+          StereoTgvImpl* s = act[k];
+          DerivPair& d = Dv.pr[k];
+          d.texI0 = s->tex1(s->pI0[level], level);
+          d.texI1w = s->tex1(s->d_i1warp, level);
+          d.tv = s->pTvF[level];
+          d.Iu = s->d_Iu;
+          d.Iz = s->d_Iz;
+          d.u = s->d_u;
+          d.u_last = s->d_u_last;
+          d.w = s->pW[level];
+          d.h = s->pH[level];
+          d.s = s->pS[level];
+          set_tiles(Dv, k, d.w, d.h);
+        }
+        Dv.npairs = na;
+        launch_derivatives_batched(Dv, st);
+      }
+      prof->profEnd();
+      float tau = 1.0f;
+      float sigma = 1.0f / tau;
+      prof->profBeginPx(kProfFused, px_level, P0.nSolverIters);
+      for (int iter = 0; iter < P0.nSolverIters; iter++) {
+        float mu;
+        if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P0.timestep_lambda);
+        else mu = 1;
+        IterArgs A{};
+        A.sigma = sigma;
+        A.tau = tau;
+        A.mu = mu;
+        A.write_tp = iter == P0.nSolverIters - 1;
+        for (int k = 0; k < na; k++) {
+          StereoTgvImpl* s = act[k];
+          IterPair& d = A.pr[k];
+          d.code = masked ? s->code_masked[level] : s->code_plain[level];
+          d.u_ = s->d_u_;
+          d.u = s->d_u;
+          d.v_ = half ? s->f_vh : (const void*)s->d_v_;
+          d.p = s->f_p;
+          d.q = s->f_q;
+          d.Tp = s->d_Tp;
+          d.a = s->d_a;
+          d.b = s->d_b;
+          d.c = s->d_c;
+          d.Iu = s->d_Iu;
+          d.Iz = s->d_Iz;
+          d.us = s->d_us;
+          d.u_s = s->d_u_s;
+          d.v_s = half ? s->f_vhs : (void*)s->d_v_s;
+          d.w = s->pW[level];
+          d.h = s->pH[level];
+          d.s = s->pS[level];
+          d.alpha0 = s->P.alpha0;
+          d.alpha1 = s->P.alpha1;
+          d.lambda = s->P.lambda;
+          // updateDualVariables.cu:174-176, 217: uniform per launch, evaluated here in float
+          A.sp[k] = s->P.alpha1 * sigma / 3.0f;
+          A.sq[k] = s->P.alpha0 * sigma / 2.0f;
+          set_iter_tiles(A, k, d.w, d.h);
+        }
+        A.npairs = na;
+        launch_fused_iteration(A, masked, half, st, iter & 1);
+        for (auto* s : act) {
+          std::swap(s->d_u, s->d_us);
+          std::swap(s->d_u_, s->d_u_s);
+          if (half) std::swap(s->f_vh, s->f_vhs);
+          else std::swap(s->d_v_, s->d_v_s);
+          s->f_parity = (iter & 1) ? 0 : 1;
+        }
+        sigma = sigma / mu;
+        tau = tau * mu;
+      }
+      prof->profEnd();
+      prof->profBeginPx(kProfEpilogue, px_level, 1);
+      {
+        EpiArgs E{};
+        E.median = masked ? 1 : 0;
+        for (int k = 0; k < na; k++) {
+          StereoTgvImpl* s = act[k];
+          EpiPair& d = E.pr[k];
+          d.u_in = s->d_u;
+          d.u_out = masked ? s->d_us : s->d_u;
+          d.u_bar = s->d_u_;
+          d.u_last = s->d_u_last;
+          d.tv2 = s->d_tv2;
+          d.warpUV = s->d_warpUV;
+          d.w = s->pW[level];
+          d.h = s->pH[level];
+          d.s = s->pS[level];
+          d.limitRange = s->P.limitRange;
+          set_tiles(E, k, d.w, d.h);
+        }
+        E.npairs = na;
+        launch_warp_epilogue_batched(E, st);
+        if (masked)
+          for (auto* s : act) std::swap(s->d_u, s->d_us);
+      }
+      prof->profEnd();
+    }
+    if (level > 0) {
+      UpArgs U{};
+      int k = 0;
+      std::vector<StereoTgvImpl*> up;
+      for (auto* s : act) {
+        UpPair& d = U.pr[k];
+        d.texU = s->tex1(s->d_u, level);
+        d.texUbar = s->tex1(s->d_u_, level);
+        d.texWarp = s->tex2(s->d_warpUV, level);
+        d.u_out = s->d_us;
+        d.ubar_out = s->d_u_s;
+        d.warp_out = s->d_warpUVs;
+        d.w = s->pW[level - 1];
+        d.h = s->pH[level - 1];
+        d.s = s->pS[level - 1];
+        d.scale = s->P.fScale;
+        set_tiles(U, k, d.w, d.h);
+        k++;
+      }
+      U.npairs = k;
+      launch_upscale_batched(U, st);
+      for (auto* s : act) {
+        std::swap(s->d_u, s->d_us);
+        std::swap(s->d_u_, s->d_u_s);
+        std::swap(s->d_warpUV, s->d_warpUVs);
+      }
+    }
+  }
+}
+
+// ---- CUDA graph of a whole batched solve ---------------------------------------------
+// The launch sequence of a solve depends only on the batch composition and on which
+// physical buffer currently plays each ping-pong role, so a captured graph is reused
+// whenever the pairs are in the same pointer state; the state after the graph is
+// recorded at capture and applied after each replay.
+PairPtrs get_ptrs(StereoTgvImpl* s) {
+  return PairPtrs{s->pI1[0], s->d_i1calibrated, s->d_u, s->d_us, s->d_u_, s->d_u_s,
+                  s->d_v_, s->d_v_s, s->d_warpUV, s->d_warpUVs, s->f_vh, s->f_vhs};
+}
+void set_ptrs(StereoTgvImpl* s, const PairPtrs& p) {
+  s->pI1[0] = p.pI1_0;
+  s->d_i1calibrated = p.i1cal;
+  s->d_u = p.u;
+  s->d_us = p.us;
+  s->d_u_ = p.u_;
+  s->d_u_s = p.u_s;
+  s->d_v_ = p.v_;
+  s->d_v_s = p.v_s;
+  s->d_warpUV = p.warpUV;
+  s->d_warpUVs = p.warpUVs;
+  s->f_vh = p.vh;
+  s->f_vhs = p.vhs;
+}
+
+FusedEngine::~FusedEngine() { clear(); }
+
+void FusedEngine::clear() {
+  for (auto& kv : cache_) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    for (auto e : kv.second.events) cudaEventDestroy(e);
+  }
+  cache_.clear();
+}
+
+void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
+  for (auto* s : pairs) {
+    if (!s->initialized()) throw ArgError{"fused solve: pair not initialized"};
+    s->ensureFused();
+    if (masked && !s->codes_valid) {
+      for (int l = 0; l < s->levels(); l++)
+        launch_edge_codes(s->pMask[l], s->code_masked[l], s->pW[l], s->pH[l], s->pS[l], s->stream());
+      s->codes_valid = true;
+    }
+  }
+}
+
+void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st) {
+  if (pairs.empty()) return;
+  prepare(pairs, masked);
+  if (!use_graph) {
+    fused_solve_direct(pairs, masked, half, st);
+    return;
+  }
+  StereoTgvImpl* prof = pairs[0];
+  std::vector<uintptr_t> key{(uintptr_t)masked, (uintptr_t)half, (uintptr_t)prof->profiling};
+  std::vector<PairPtrs> before;
+  for (auto* s : pairs) {
+    PairPtrs p = get_ptrs(s);
+    before.push_back(p);
+    const uintptr_t* w = reinterpret_cast<const uintptr_t*>(&p);
+    key.push_back((uintptr_t)s);
+    key.push_back((uintptr_t)s->generation);
+    key.insert(key.end(), w, w + sizeof(PairPtrs) / sizeof(uintptr_t));
+    uint32_t lr;
+    std::memcpy(&lr, &s->P.limitRange, 4);
+    key.push_back(lr);
+  }
+  auto it = cache_.find(key);
+  if (it == cache_.end()) {
+    Entry e;
+    std::vector<ProfRec> saved = prof->profRecords();
+    prof->profReset();
+    prof->capture_events = &e.events;
+    cudaGraph_t g = nullptr;
+    VFS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+    try {
+      fused_solve_direct(pairs, masked, half, st);
+    } catch (...) {
+      prof->capture_events = nullptr;
+      cudaGraph_t junk = nullptr;
+      cudaStreamEndCapture(st, &junk);
+      if (junk) cudaGraphDestroy(junk);
+      for (auto ev : e.events) cudaEventDestroy(ev);
+      for (size_t k = 0; k < pairs.size(); k++) set_ptrs(pairs[k], before[k]);
+      throw;
+    }
+    prof->capture_events = nullptr;
+    VFS_CUDA(cudaStreamEndCapture(st, &g));
+    cudaError_t ie = cudaGraphInstantiate(&e.exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) throw CudaError{ie, "cudaGraphInstantiate", __FILE__, __LINE__};
+    for (auto* s : pairs) e.after.push_back(get_ptrs(s));
+    e.prof = prof->profRecords();
+    prof->setProfRecords(saved);
+    for (size_t k = 0; k < pairs.size(); k++) set_ptrs(pairs[k], before[k]);
+    it = cache_.emplace(key, std::move(e)).first;
+  }
+  VFS_CUDA(cudaGraphLaunch(it->second.exec, st));
+  for (size_t k = 0; k < pairs.size(); k++) set_ptrs(pairs[k], it->second.after[k]);
+  if (prof->profiling) prof->setProfRecords(it->second.prof);
+}
+
+}  // namespace vfs

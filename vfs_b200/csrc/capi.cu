@@ -11,6 +11,23 @@
 #include "io.hpp"
 #include "stereo_tgv.cuh"
 
+struct vfs_batch {
+  std::vector<vfs_stereo*> members;
+  vfs::FusedEngine engine;
+  cudaStream_t stream = 0;      // the batch's stream (its own unless set)
+  cudaStream_t own = nullptr;
+  cudaEvent_t done = nullptr;   // batch work finished (members' streams wait on it)
+  std::vector<cudaEvent_t> ready;  // member work finished (the batch stream waits on them)
+  bool half = false;
+  std::string err;
+  ~vfs_batch() {
+    engine.clear();
+    for (auto e : ready) cudaEventDestroy(e);
+    if (done) cudaEventDestroy(done);
+    if (own) cudaStreamDestroy(own);
+  }
+};
+
 struct vfs_stereo {
   vfs::StereoTgvImpl impl;
   std::string err;
@@ -28,8 +45,8 @@ namespace {
 
 thread_local std::string g_create_error;
 
-template <class F>
-int guarded(vfs_stereo* s, F&& f) {
+template <class H, class F>
+int guarded(H* s, F&& f) {
   if (!s) return VFS_ERR_ARG;
   try {
     f();
@@ -219,6 +236,124 @@ int vfs_debug_get_buffer(vfs_stereo* s, const char* name, int comps, float* out)
   return guarded(s, [&] {
     if (!name || !out) throw vfs::ArgError{"debug get: null argument"};
     s->impl.debugGet(name, comps, out);
+  });
+}
+
+int vfs_set_solve_path(vfs_stereo* s, int path, int half_storage) {
+  return guarded(s, [&] {
+    if (path != VFS_PATH_REFERENCE && path != VFS_PATH_FUSED) throw vfs::ArgError{"unknown solve path"};
+    if (path == VFS_PATH_REFERENCE && half_storage) throw vfs::ArgError{"half storage needs the fused path"};
+    s->impl.path = path == VFS_PATH_FUSED ? vfs::SolvePath::kFused : vfs::SolvePath::kReference;
+    s->impl.half_storage = half_storage != 0;
+  });
+}
+
+int vfs_set_graph(vfs_stereo* s, int use_graph) {
+  return guarded(s, [&] { s->impl.engine.use_graph = use_graph != 0; });
+}
+
+int vfs_batch_create(vfs_batch** out) {
+  if (!out) return VFS_ERR_ARG;
+  *out = new (std::nothrow) vfs_batch();
+  if (!*out) return VFS_ERR_NOMEM;
+  if (cudaStreamCreateWithFlags(&(*out)->own, cudaStreamNonBlocking) != cudaSuccess) {
+    (void)cudaGetLastError();
+    delete *out;
+    *out = nullptr;
+    return VFS_ERR_CUDA;
+  }
+  (*out)->stream = (*out)->own;
+  return VFS_OK;
+}
+
+int vfs_batch_destroy(vfs_batch* b) {
+  if (!b) return VFS_ERR_ARG;
+  cudaStreamSynchronize(b->stream);
+  delete b;
+  return VFS_OK;
+}
+
+const char* vfs_batch_last_error(const vfs_batch* b) { return b ? b->err.c_str() : ""; }
+
+int vfs_batch_set_stream(vfs_batch* b, void* st) {
+  return guarded(b, [&] {
+    VFS_CUDA(cudaStreamSynchronize(b->stream));
+    b->stream = st ? (cudaStream_t)st : b->own;
+    b->engine.clear();
+  });
+}
+
+int vfs_batch_add(vfs_batch* b, vfs_stereo* s) {
+  return guarded(b, [&] {
+    if (!s) throw vfs::ArgError{"batch add: null handle"};
+    if ((int)b->members.size() >= vfs::kMaxPairs) throw vfs::ArgError{"batch is full"};
+    for (auto* m : b->members)
+      if (m == s) throw vfs::ArgError{"batch add: handle already in the batch"};
+    if (!s->impl.initialized()) throw vfs::ArgError{"batch add: handle not initialized"};
+    cudaEvent_t e;
+    VFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->ready.push_back(e);
+    b->members.push_back(s);
+    b->engine.clear();
+  });
+}
+
+int vfs_batch_clear(vfs_batch* b) {
+  return guarded(b, [&] {
+    VFS_CUDA(cudaStreamSynchronize(b->stream));
+    b->members.clear();
+    b->engine.clear();
+  });
+}
+
+int vfs_batch_size(const vfs_batch* b) { return b ? (int)b->members.size() : VFS_ERR_ARG; }
+
+int vfs_batch_set_storage(vfs_batch* b, int half) {
+  return guarded(b, [&] { b->half = half != 0; });
+}
+
+int vfs_batch_set_graph(vfs_batch* b, int use_graph) {
+  return guarded(b, [&] { b->engine.use_graph = use_graph != 0; });
+}
+
+int vfs_batch_solve(vfs_batch* b, int masked) {
+  return guarded(b, [&] {
+    if (b->members.empty()) throw vfs::ArgError{"batch solve: empty batch"};
+    std::vector<vfs::StereoTgvImpl*> pairs;
+    for (auto* m : b->members) pairs.push_back(&m->impl);
+    // per-pair preparation on each member's own stream, then order the batch stream
+    // after every member's queued work and every member's stream after the batch
+    vfs::FusedEngine::prepare(pairs, masked != 0);
+    if (!b->done) VFS_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+    for (size_t k = 0; k < pairs.size(); k++) {
+      if (pairs[k]->stream() == b->stream) continue;
+      VFS_CUDA(cudaEventRecord(b->ready[k], pairs[k]->stream()));
+      VFS_CUDA(cudaStreamWaitEvent(b->stream, b->ready[k], 0));
+    }
+    b->engine.solve(pairs, masked != 0, b->half, b->stream);
+    VFS_CUDA(cudaEventRecord(b->done, b->stream));
+    for (auto* p : pairs)
+      if (p->stream() != b->stream) VFS_CUDA(cudaStreamWaitEvent(p->stream(), b->done, 0));
+  });
+}
+
+long long vfs_launch_count(void) { return vfs::launch_counter().load(); }
+
+int vfs_profile_enable(vfs_stereo* s, int on) {
+  return guarded(s, [&] { s->impl.profiling = on != 0; });
+}
+
+int vfs_profile_reset(vfs_stereo* s) {
+  return guarded(s, [&] {
+    VFS_CUDA(cudaStreamSynchronize(s->impl.stream()));
+    s->impl.profReset();
+  });
+}
+
+int vfs_profile_read(vfs_stereo* s, int kind, long long* n, double* ms, double* pi) {
+  return guarded(s, [&] {
+    if (kind < 0 || kind >= vfs::kProfTags) throw vfs::ArgError{"profile kind out of range"};
+    s->impl.profRead(kind, n, ms, pi);
   });
 }
 

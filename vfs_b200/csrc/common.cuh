@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
 #include <map>
 #include <string>
@@ -24,7 +25,24 @@ struct CudaError {
     if (e_ != cudaSuccess) throw ::vfs::CudaError{e_, #call, __FILE__, __LINE__}; \
   } while (0)
 
-#define VFS_LAUNCH_CHECK() VFS_CUDA(cudaGetLastError())
+// Every kernel launch of the library goes through VFS_LAUNCH_CHECK, which also
+// counts it (vfs_launch_count in the C ABI).
+std::atomic<long long>& launch_counter();
+#define VFS_LAUNCH_CHECK()                                                  \
+  do {                                                                      \
+    VFS_CUDA(cudaGetLastError());                                           \
+    ::vfs::launch_counter().fetch_add(1, std::memory_order_relaxed);        \
+  } while (0)
+
+// Opt-in timing of launch groups with CUDA events on the solver's stream.
+struct ProfRec {
+  int tag;        // ProfTag
+  int level;
+  long long px;   // pixels of the level
+  int iters;      // inner iterations covered by the record
+  cudaEvent_t a, b;
+};
+enum ProfTag { kProfInner = 0, kProfFused = 1, kProfPrologue = 2, kProfEpilogue = 3, kProfTags = 4 };
 
 struct ArgError {
   std::string msg;

@@ -1,0 +1,190 @@
+// Fused, batched kernels of the fast solve path.
+//
+// One launch covers every pair of a batch at one pyramid level; pairs may differ in
+// size.  Per-pair state is passed by value in the kernel parameters (up to
+// kMaxPairs pairs), with the pointers that are current at that launch, so a launch
+// sequence can be captured once in a CUDA graph and replayed.
+//
+// With float storage the fused kernels compute bit-for-bit what the per-kernel
+// drop-in path computes: the same operations in the same order on the same
+// physical buffers (including the stale values that masked-out pixels keep), so
+// the two paths agree exactly.  With half storage p, q and v-bar are kept as
+// IEEE half in memory and widened to float for all arithmetic.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace vfs {
+
+constexpr int kMaxPairs = 24;
+constexpr int kFTW = 32;  // fused iteration tile: 32 x 8 pixels, one thread each
+constexpr int kFTH = 8;
+
+// per-level edge code of each pixel (computed once per mask upload):
+//   bit0 mask(x) != 0, bit1 right neighbour on, bit2 left on, bit3 down on, bit4 up on
+// (a neighbour outside the image counts as off, as in the reference's masked kernels)
+enum : uint8_t { kOn = 1, kR = 2, kL = 4, kD = 8, kU = 16 };
+
+template <class ST>
+struct Store2;  // storage of a 2-vector (p, v-bar) and a 4-vector (q)
+template <>
+struct Store2<float> {
+  typedef float2 T2;
+  typedef float4 T4;
+  static __device__ __forceinline__ float2 ld2(const T2* b, long long k) { return b[k]; }
+  static __device__ __forceinline__ void st2(T2* b, long long k, float2 v) { b[k] = v; }
+  static __device__ __forceinline__ float4 ld4(const T4* b, long long k) { return b[k]; }
+  static __device__ __forceinline__ void st4(T4* b, long long k, float4 v) { b[k] = v; }
+};
+template <>
+struct Store2<__half> {
+  typedef __half2 T2;
+  struct __align__(8) T4 { __half2 a, b; };
+  static __device__ __forceinline__ float2 ld2(const T2* b, long long k) { return __half22float2(b[k]); }
+  static __device__ __forceinline__ void st2(T2* b, long long k, float2 v) { b[k] = __float22half2_rn(v); }
+  static __device__ __forceinline__ float4 ld4(const T4* b, long long k) {
+    T4 t = b[k];
+    float2 x = __half22float2(t.a), y = __half22float2(t.b);
+    return make_float4(x.x, x.y, y.x, y.y);
+  }
+  static __device__ __forceinline__ void st4(T4* b, long long k, float4 v) {
+    T4 t;
+    t.a = __float22half2_rn(make_float2(v.x, v.y));
+    t.b = __float22half2_rn(make_float2(v.z, v.w));
+    b[k] = t;
+  }
+};
+
+// ---- one primal-dual iteration -------------------------------------------------
+struct IterPair {
+  const uint8_t* code;  // edge codes (masked form) or inside-circle flags (plain form)
+  const float* u_;      // u-bar (current)
+  const float* u;       // u (current)
+  const void* v_;       // v-bar (current), Store2<ST>::T2
+  void* p;              // T2, in place
+  void* q;              // T4, in place
+  float2* Tp;           // T p (float); read for masked-out neighbours, written when write_tp
+  const float *a, *b, *c, *Iu, *Iz;
+  float* us;            // thresholded u (output)
+  float* u_s;           // new u-bar (output)
+  void* v_s;            // new v-bar (output), T2
+  int w, h, s, tiles_x, tile0;
+  float alpha0, alpha1, lambda;
+};
+struct IterArgs {
+  int npairs, ntiles;
+  float sigma, tau, mu;
+  float sp[kMaxPairs], sq[kMaxPairs];  // alpha1 sigma / 3 and alpha0 sigma / 2 per pair (host-evaluated)
+  int write_tp;
+  IterPair pr[kMaxPairs];
+};
+// parity selects which half of the p / q ping-pong buffers is read (the other is written)
+void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity);
+
+// ---- per-warp prologue: zero p, q, v-bar; resample tv at x + warpUV; warp I1 ----
+struct WarpStartPair {
+  cudaTextureObject_t texI1, texTv;
+  const float2* warpUV;
+  float2* tv2;
+  float* i1warp;
+  void *p, *q, *v_;  // zeroed (px < w); storage type by half_storage
+  int w, h, s, tiles_x, tile0;
+};
+struct WarpStartArgs {
+  int npairs, ntiles;
+  WarpStartPair pr[kMaxPairs];
+};
+void launch_warp_start(const WarpStartArgs& A, bool half_storage, cudaStream_t st);
+
+// ---- derivatives along the translation field + u_last = u -----------------------
+struct DerivPair {
+  cudaTextureObject_t texI0, texI1w;
+  const float2* tv;
+  float *Iu, *Iz;
+  const float* u;
+  float* u_last;
+  int w, h, s, tiles_x, tile0;
+};
+struct DerivArgs {
+  int npairs, ntiles;
+  DerivPair pr[kMaxPairs];
+};
+void launch_derivatives_batched(const DerivArgs& A, cudaStream_t st);
+
+// ---- 5x5 median (masked form) + range limit + u / u-bar / warpUV update ----------
+struct EpiPair {
+  const float* u_in;   // u after the inner loop (median input)
+  float* u_out;        // receives u_last + min(median - u_last, limit)
+  float* u_bar;        // u-bar = u
+  const float* u_last;
+  const float2* tv2;
+  float2* warpUV;      // += du * tv2
+  int w, h, s, tiles_x, tile0;
+  float limitRange;
+};
+struct EpiArgs {
+  int npairs, ntiles;
+  int median;  // 1: masked form applies the 5x5 median first
+  EpiPair pr[kMaxPairs];
+};
+void launch_warp_epilogue_batched(const EpiArgs& A, cudaStream_t st);
+
+// ---- per-level setup: gaussian (+ zero where not computed), tensor (+ zero) -------
+struct LevelPair {
+  cudaTextureObject_t texI0, texSmooth;
+  const float* mask;  // nullptr: plain form
+  float* i0smooth;
+  float *a, *b, *c;
+  float2* warpUV;        // coarsest level: warpUV = u * tv (u = 0)
+  const float* u;
+  const float2* tv;
+  int init_flow;         // 1 at a pair's coarsest level
+  int w, h, s, xmax, tiles_x, tile0;
+  float beta, gamma;
+};
+struct LevelArgs {
+  int npairs, ntiles;
+  LevelPair pr[kMaxPairs];
+};
+void launch_level_gaussian(const LevelArgs& A, cudaStream_t st);
+void launch_level_tensor(const LevelArgs& A, cudaStream_t st);
+
+// ---- upscale u, u-bar and warpUV to the next finer level in one pass --------------
+struct UpPair {
+  cudaTextureObject_t texU, texUbar, texWarp;
+  float *u_out, *ubar_out;
+  float2* warp_out;
+  int w, h, s, tiles_x, tile0;  // fine level
+  float scale;
+};
+struct UpArgs {
+  int npairs, ntiles;
+  UpPair pr[kMaxPairs];
+};
+void launch_upscale_batched(const UpArgs& A, cudaStream_t st);
+
+// ---- pyramid: downscale I0 and I1 of every pair to the next coarser level --------
+struct DownPair {
+  cudaTextureObject_t texI0, texI1;
+  float *I0, *I1;
+  int w, h, s, tiles_x, tile0;  // coarse level
+};
+struct DownArgs {
+  int npairs, ntiles;
+  DownPair pr[kMaxPairs];
+};
+void launch_downscale_batched(const DownArgs& A, cudaStream_t st);
+
+// edge codes of one level from its mask (masked form) or the fixed circle (plain)
+void launch_edge_codes(const float* mask, uint8_t* code, int w, int h, int s, cudaStream_t st);
+
+// tile bookkeeping shared by the batched launches (32 x 8 tiles)
+inline int tiles_x_of(int w) { return (w + kFTW - 1) / kFTW; }
+inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFTH); }
+// the iteration kernel's tiles: 31 x kIterTH pixels (a 32 x (kIterTH + 1) block with halo)
+constexpr int kIterTH = 8;
+inline int iter_tiles_x_of(int w) { return (w + 30) / 31; }
+inline int iter_tiles_of(int w, int h) { return iter_tiles_x_of(w) * ((h + kIterTH - 1) / kIterTH); }
+
+}  // namespace vfs

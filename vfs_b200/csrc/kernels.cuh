@@ -49,6 +49,7 @@ struct DualArgs {
   float2* p;
   float4* q;
   float alpha0, alpha1, sigma, eta_p, eta_q;
+  float sp, sq;  // alpha1 * sigma / eta_p and alpha0 * sigma / eta_q (set by the launcher)
 };
 // updateDualVariables.cu:4-101 / :122-237
 void launch_update_dual(const DualArgs& A, Geom g, cudaStream_t st);

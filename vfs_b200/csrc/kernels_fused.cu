@@ -1,0 +1,442 @@
+// Fused, batched kernels of the fast solve path (see fused.cuh).
+#include "common.cuh"
+#include "fused.cuh"
+#include "tgv_math.cuh"
+#include "tgv_pixel.cuh"
+
+namespace vfs {
+
+// Locate the pair and the 32 x 8 tile of this block from the batch's tile ranges.
+template <class PairT, int N>
+__device__ __forceinline__ int find_pair(const PairT (&pr)[N], int npairs, int t) {
+  int k = 0;
+  while (k + 1 < npairs && t >= pr[k + 1].tile0) k++;
+  return k;
+}
+
+#define TILE_SETUP(ARGS)                                        \
+  const int t_ = blockIdx.x;                                    \
+  const int pi_ = find_pair(ARGS.pr, ARGS.npairs, t_);          \
+  const auto& P = ARGS.pr[pi_];                                 \
+  const int lt_ = t_ - P.tile0;                                 \
+  const int x0 = (lt_ % P.tiles_x) * kFTW;                      \
+  const int y0 = (lt_ / P.tiles_x) * kFTH;                      \
+  const int ix = x0 + (int)threadIdx.x;                         \
+  const int iy = y0 + (int)threadIdx.y;
+
+// ---------------------------------------------------------------------------
+// One primal-dual iteration (updateDualVariables + solveTp + thresholdingL1 +
+// updatePrimalVariables).  The dual update is also evaluated on a one-pixel halo to
+// the left and top of the tile (the threshold and primal steps read T p and q of the
+// west and north neighbours), so p and q are read from one buffer and written to
+// another (the caller ping-pongs them).
+// ---------------------------------------------------------------------------
+template <bool MASKED, class ST>
+struct FusedIter {
+  typedef Store2<ST> S;
+  typedef typename S::T2 T2;
+  typedef typename S::T4 T4;
+
+  // dual update at an in-image pixel; returns false where the pixel keeps its
+  // values (masked out), in which case tp is the stored (stale) T p.
+  static __device__ __forceinline__ bool dual_at(const IterPair& P, const T2* pin, const T4* qin, int ix, int iy,
+                                                 float sp, float sq, float2& p, float4& q, float2& tp) {
+    int pos = ix + iy * P.s;
+    int right = pos + 1, down = pos + P.s, left = pos - 1, up = pos - P.s;
+    bool useRight, useDown;
+    uint8_t code = P.code[pos];
+    float a = P.a[pos], b = P.b[pos], c = P.c[pos];
+    if (MASKED) {
+      if (!(code & kOn)) {
+        tp = P.Tp[pos];
+        return false;
+      }
+      useRight = code & kR;
+      useDown = code & kD;
+    } else {
+      if (!(code & kOn)) {  // outside the circle: p = q = 0, T p = T 0
+        p = make_float2(0.f, 0.f);
+        q = make_float4(0.f, 0.f, 0.f, 0.f);
+        tp = tp_math(a, b, c, p);
+        return true;
+      }
+      useRight = (ix + 1) < P.w;
+      useDown = (iy + 1) < P.h;
+    }
+    const T2* v_ = (const T2*)P.v_;
+    float u_pos = P.u_[pos];
+    float2 vp = S::ld2(v_, pos);
+    float u_xn = useRight ? P.u_[right] : (left < 0 ? 0.0f : P.u_[left]);
+    float u_yn = useDown ? P.u_[down] : (up < 0 ? 0.0f : P.u_[up]);
+    float2 v_xn = useRight ? S::ld2(v_, right) : (left < 0 ? make_float2(0.f, 0.f) : S::ld2(v_, left));
+    float2 v_yn = useDown ? S::ld2(v_, down) : (up < 0 ? make_float2(0.f, 0.f) : S::ld2(v_, up));
+    p = S::ld2(pin, pos);
+    q = S::ld4(qin, pos);
+    dual_math(useRight, useDown, u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
+    tp = tp_math(a, b, c, p);
+    return true;
+  }
+};
+
+// The block is a 32 x (TH + 1) region: one image row segment per warp, the first
+// column and the first row being the halo of the 31 x TH tile.  Every thread
+// evaluates the dual update at its region pixel; after a barrier the tile threads
+// finish the threshold and primal steps with the west / north values from shared
+// memory.
+template <bool MASKED, class ST, int TH>
+__global__ void __launch_bounds__(32 * (TH + 1)) k_fused_iter(const __grid_constant__ IterArgs A, int parity) {
+  typedef FusedIter<MASKED, ST> F;
+  typedef typename F::T2 T2;
+  typedef typename F::T4 T4;
+  typedef Store2<ST> S;
+  __shared__ float2 sTp[TH + 1][32];
+  __shared__ float4 sQ[TH + 1][32];
+  const int t_ = blockIdx.x;
+  const int pi_ = find_pair(A.pr, A.npairs, t_);
+  const IterPair& P = A.pr[pi_];
+  const int lt_ = t_ - P.tile0;
+  const int x0 = (lt_ % P.tiles_x) * 31;
+  const int y0 = (lt_ / P.tiles_x) * TH;
+  const int rx = threadIdx.x, ry = threadIdx.y;
+  const int ix = x0 - 1 + rx, iy = y0 - 1 + ry;
+  const int plane = P.s * P.h;
+  const T2* pin = (const T2*)P.p + (parity ? plane : 0);
+  const T4* qin = (const T4*)P.q + (parity ? plane : 0);
+  T2* pout = (T2*)P.p + (parity ? 0 : plane);
+  T4* qout = (T4*)P.q + (parity ? 0 : plane);
+  const bool tile = rx >= 1 && ry >= 1;
+  const bool in_img = ix >= 0 && iy >= 0 && ix < P.w && iy < P.h;
+  const int pos = ix + iy * P.s;
+
+  // ---- phase 1: dual update at every region pixel ------------------------------------
+  float2 pp = make_float2(0.f, 0.f), tp = make_float2(0.f, 0.f);
+  float4 qq = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (in_img) {
+    bool own = F::dual_at(P, pin, qin, ix, iy, A.sp[pi_], A.sq[pi_], pp, qq, tp);
+    if (own && tile) {
+      S::st2(pout, pos, pp);
+      S::st4(qout, pos, qq);
+      if (A.write_tp) P.Tp[pos] = tp;
+    }
+  } else if (ix < 0 && iy >= 1 && iy < P.h) {
+    // left of the image: the reference's west neighbour of column 0 is the flat
+    // position before it, the last padding element of the previous row (row 0 has
+    // none; positions before the buffer start read 0).  Halo pixels right of or
+    // below the image are never read.
+    tp = P.Tp[pos];
+  }
+  sTp[ry][rx] = tp;
+  sQ[ry][rx] = qq;
+  __syncthreads();
+  if (!tile || !in_img) return;
+  uint8_t code = P.code[pos];
+  float a = P.a[pos], b = P.b[pos], c = P.c[pos];
+
+  // ---- phase 2: thresholding --------------------------------------------------------
+  float dxm, dym;
+  bool zR, zD, hasL, hasU;
+  if (MASKED) {
+    if (!(code & kOn)) return;
+    bool mR = code & kR, mL = code & kL, mD = code & kD, mU = code & kU;
+    if (mL && mR) dxm = tp.x - sTp[ry][rx - 1].x;
+    else if (!mR) dxm = -sTp[ry][rx - 1].x;
+    else dxm = tp.x;
+    if (mU && mD) dym = tp.y - sTp[ry - 1][rx].y;
+    else if (!mD) dym = -sTp[ry - 1][rx].y;
+    else dym = tp.y;
+    zR = !mR;
+    zD = !mD;
+    hasL = mL;
+    hasU = mU;
+  } else {
+    if (!(code & kOn)) {
+      P.us[pos] = 0.0f;
+      P.u_s[pos] = 0.0f;
+      S::st2((T2*)P.v_s, pos, make_float2(0.f, 0.f));
+      return;
+    }
+    if ((ix - 1) >= 0) dxm = tp.x - sTp[ry][rx - 1].x;
+    else if (ix == P.w - 1) dxm = -sTp[ry][rx - 1].x;
+    else dxm = tp.x;
+    if ((iy - 1) >= 0) dym = tp.y - sTp[ry - 1][rx].y;
+    else if (iy == P.h - 1) dym = -sTp[ry - 1][rx].y;
+    else dym = tp.y;
+    zR = ix == P.w - 1;
+    zD = iy == P.h - 1;
+    hasL = (ix - 1) >= 0;
+    hasU = (iy - 1) >= 0;
+  }
+  float ubar = P.u_[pos];
+  float eu = etau_math(a, b, c, P.alpha1);
+  float unew = threshold_math(dxm, dym, eu, A.tau, ubar, P.u[pos], P.Iu[pos], P.Iz[pos], P.lambda);
+  P.us[pos] = unew;
+
+  // ---- phase 3: primal update ------------------------------------------------------
+  float4 qc = qq;
+  if (zR) qc.x = qc.w = 0.0f;
+  if (zD) qc.y = qc.z = 0.0f;
+  float4 ql = hasL ? sQ[ry][rx - 1] : make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 qu = hasU ? sQ[ry - 1][rx] : make_float4(0.f, 0.f, 0.f, 0.f);
+  float ev1 = etav1_math(b, c, P.alpha0, P.alpha1), ev2 = etav2_math(a, c, P.alpha0, P.alpha1);
+  float2 vb = S::ld2((const T2*)P.v_, pos);
+  float us_;
+  float2 vs, vo;
+  primal_math(qc, ql, qu, pp, a, b, c, ev1, ev2, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs, vo);
+  P.u_s[pos] = us_;
+  S::st2((T2*)P.v_s, pos, vs);
+}
+
+void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity) {
+  constexpr int TH = kIterTH;
+  dim3 blk(32, TH + 1);
+  if (A.ntiles <= 0) return;
+  if (masked) {
+    if (half_storage) k_fused_iter<true, __half, TH><<<A.ntiles, blk, 0, st>>>(A, parity);
+    else k_fused_iter<true, float, TH><<<A.ntiles, blk, 0, st>>>(A, parity);
+  } else {
+    if (half_storage) k_fused_iter<false, __half, TH><<<A.ntiles, blk, 0, st>>>(A, parity);
+    else k_fused_iter<false, float, TH><<<A.ntiles, blk, 0, st>>>(A, parity);
+  }
+  VFS_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Per-warp prologue: zero p, q (both halves) and v-bar; tv2 = tv(x + warpUV);
+// i1warp = I1(x + warpUV)  (stereotgv.cu:431-439; warpImage.cu:9-23, 96-111)
+// ---------------------------------------------------------------------------
+template <class ST>
+__global__ void __launch_bounds__(kFTW* kFTH) k_warp_start(const __grid_constant__ WarpStartArgs A) {
+  typedef Store2<ST> S;
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  long long pos = ix + (long long)iy * P.s;
+  long long plane = (long long)P.s * P.h;
+  typename S::T2* p = (typename S::T2*)P.p;
+  typename S::T4* q = (typename S::T4*)P.q;
+  S::st2(p, pos, make_float2(0.f, 0.f));
+  S::st2(p, pos + plane, make_float2(0.f, 0.f));
+  S::st4(q, pos, make_float4(0.f, 0.f, 0.f, 0.f));
+  S::st4(q, pos + plane, make_float4(0.f, 0.f, 0.f, 0.f));
+  S::st2((typename S::T2*)P.v_, pos, make_float2(0.f, 0.f));
+  float2 wv = P.warpUV[pos];
+  float x = ((float)ix + wv.x + 0.5f) / (float)P.w;
+  float y = ((float)iy + wv.y + 0.5f) / (float)P.h;
+  P.tv2[pos] = tex2D<float2>(P.texTv, x, y);
+  P.i1warp[pos] = tex2D<float>(P.texI1, x, y);
+}
+
+void launch_warp_start(const WarpStartArgs& A, bool half_storage, cudaStream_t st) {
+  if (A.ntiles <= 0) return;
+  dim3 blk(kFTW, kFTH);
+  if (half_storage) k_warp_start<__half><<<A.ntiles, blk, 0, st>>>(A);
+  else k_warp_start<float><<<A.ntiles, blk, 0, st>>>(A);
+  VFS_LAUNCH_CHECK();
+}
+
+// computeDerivatives.cu:89-129 and Clone(u_last, u) (stereotgv.cu:447)
+__global__ void __launch_bounds__(kFTW* kFTH) k_derivatives_b(const __grid_constant__ DerivArgs A) {
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  long long pos = ix + (long long)iy * P.s;
+  float2 vv = P.tv[pos];
+  float r = sqrtf(vv.x * vv.x + vv.y * vv.y);
+  float dx = (vv.x / r) / (float)P.w;
+  float dy = (vv.y / r) / (float)P.h;
+  float x = ((float)ix + 0.5f) / (float)P.w;
+  float y = ((float)iy + 0.5f) / (float)P.h;
+  cudaTextureObject_t I0 = P.texI0, I1 = P.texI1w;
+  float t0 = tex2D<float>(I0, x - 2.0f * dx, y - 2.0f * dy);
+  t0 -= tex2D<float>(I0, x - 1.0f * dx, y - 1.0f * dy) * 8.0f;
+  t0 += tex2D<float>(I0, x + 1.0f * dx, y + 1.0f * dy) * 8.0f;
+  t0 -= tex2D<float>(I0, x + 2.0f * dx, y + 2.0f * dy);
+  t0 /= 12.0f;
+  float t1 = tex2D<float>(I1, x - 2.0f * dx, y - 2.0f * dy);
+  t1 -= tex2D<float>(I1, x - 1.0f * dx, y - 1.0f * dy) * 8.0f;
+  t1 += tex2D<float>(I1, x + 1.0f * dx, y + 1.0f * dy) * 8.0f;
+  t1 -= tex2D<float>(I1, x + 2.0f * dx, y + 2.0f * dy);
+  t1 /= 12.0f;
+  P.Iu[pos] = (t0 + t1) * 0.5f;
+  P.Iz[pos] = tex2D<float>(I1, x, y) - tex2D<float>(I0, x, y);
+  P.u_last[pos] = P.u[pos];
+}
+
+void launch_derivatives_batched(const DerivArgs& A, cudaStream_t st) {
+  if (A.ntiles <= 0) return;
+  k_derivatives_b<<<A.ntiles, dim3(kFTW, kFTH), 0, st>>>(A);
+  VFS_LAUNCH_CHECK();
+}
+
+// stereotgv.cu:481-493: median (masked form), du = min(u - u_last, limit),
+// u = u_last + du, u-bar = u, warpUV += du * tv2
+__global__ void __launch_bounds__(kFTW* kFTH) k_epilogue_b(const __grid_constant__ EpiArgs A) {
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  long long pos = ix + (long long)iy * P.s;
+  float m = A.median ? median5_at(P.u_in, ix, iy, P.w, P.h, P.s) : P.u_in[pos];
+  float ul = P.u_last[pos];
+  float d = m - ul;
+  d = d > P.limitRange ? P.limitRange : d;
+  float un = ul + d;
+  P.u_out[pos] = un;
+  P.u_bar[pos] = un;
+  float2 t = P.tv2[pos];
+  float2 dw = make_float2(d * t.x, d * t.y);
+  float2 wv = P.warpUV[pos];
+  P.warpUV[pos] = make_float2(wv.x + dw.x, wv.y + dw.y);
+}
+
+void launch_warp_epilogue_batched(const EpiArgs& A, cudaStream_t st) {
+  if (A.ntiles <= 0) return;
+  k_epilogue_b<<<A.ntiles, dim3(kFTW, kFTH), 0, st>>>(A);
+  VFS_LAUNCH_CHECK();
+}
+
+// calcTensor.cu:99-128 / 245-273 with the per-level zeroing of stereotgv.cu:409-415:
+// i0smooth = gaussian where computed, 0 elsewhere (level footprint); at a pair's
+// coarsest level also warpUV = u * tv (stereotgv.cu:419-421).
+__global__ void __launch_bounds__(kFTW* kFTH) k_level_gaussian(const __grid_constant__ LevelArgs A) {
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  long long pos = ix + (long long)iy * P.s;
+  if (P.init_flow) {
+    float us = P.u[pos];
+    float2 t = P.tv[pos];
+    P.warpUV[pos] = make_float2(us * t.x, us * t.y);
+  }
+  if (P.mask && P.mask[pos] == 0.0f) {
+    P.i0smooth[pos] = 0.0f;
+    return;
+  }
+  float dx = 1.0f / (float)P.w, dy = 1.0f / (float)P.h;
+  float x = ((float)ix + 0.5f) * dx, y = ((float)iy + 0.5f) * dy;
+  cudaTextureObject_t in = P.texI0;
+  float t0 = (1 / 4.0f) * tex2D<float>(in, x, y);
+  t0 += (1 / 16.0f) * tex2D<float>(in, x - 1.0f * dx, y - 1.0f * dy);
+  t0 += (1 / 16.0f) * tex2D<float>(in, x - 1.0f * dx, y + 1.0f * dy);
+  t0 += (1 / 16.0f) * tex2D<float>(in, x + 1.0f * dx, y - 1.0f * dy);
+  t0 += (1 / 16.0f) * tex2D<float>(in, x + 1.0f * dx, y + 1.0f * dy);
+  t0 += (1 / 8.0f) * tex2D<float>(in, x - 1.0f * dx, y);
+  t0 += (1 / 8.0f) * tex2D<float>(in, x + 1.0f * dx, y);
+  t0 += (1 / 8.0f) * tex2D<float>(in, x, y - 1.0f * dy);
+  t0 += (1 / 8.0f) * tex2D<float>(in, x, y + 1.0f * dy);
+  P.i0smooth[pos] = t0;
+}
+
+// calcTensor.cu:8-73 / 155-219; a = b = c = 0 where the reference does not compute
+// (masked out, or columns >= xmax of its launch grid)
+__global__ void __launch_bounds__(kFTW* kFTH) k_level_tensor(const __grid_constant__ LevelArgs A) {
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  long long pos = ix + (long long)iy * P.s;
+  if (ix >= P.xmax || (P.mask && P.mask[pos] == 0.0f)) {
+    P.a[pos] = 0.0f;
+    P.b[pos] = 0.0f;
+    P.c[pos] = 0.0f;
+    return;
+  }
+  float dx = 1.0f / (float)P.w, dy = 1.0f / (float)P.h;
+  float x = ((float)ix + 0.5f) * dx, y = ((float)iy + 0.5f) * dy;
+  cudaTextureObject_t gray = P.texSmooth;
+  float gx = tex2D<float>(gray, x + 1.0f * dx, y + 1.0f * dy) - tex2D<float>(gray, x, y + 1.0f * dy);
+  float gy = tex2D<float>(gray, x + 1.0f * dx, y + 1.0f * dy) - tex2D<float>(gray, x + 1.0f * dx, y);
+  float abs_img = sqrtf(gx * gx + gy * gy);
+  float norm_n = abs_img;
+  float nx = gx / norm_n, ny = gy / norm_n;
+  if (norm_n < 1e-8f) {
+    nx = 1.0f;
+    ny = 0.0f;
+  }
+  float ntx = ny, nty = -nx;
+  float wt = tgv_exp(-P.beta * tgv_pow(abs_img, P.gamma));
+  if (!(wt > 1e-8f)) wt = 1e-8f;
+  P.a[pos] = wt * nx * nx + ntx * ntx;
+  P.c[pos] = wt * nx * ny + ntx * nty;
+  P.b[pos] = wt * ny * ny + nty * nty;
+}
+
+void launch_level_gaussian(const LevelArgs& A, cudaStream_t st) {
+  if (A.ntiles <= 0) return;
+  k_level_gaussian<<<A.ntiles, dim3(kFTW, kFTH), 0, st>>>(A);
+  VFS_LAUNCH_CHECK();
+}
+void launch_level_tensor(const LevelArgs& A, cudaStream_t st) {
+  if (A.ntiles <= 0) return;
+  k_level_tensor<<<A.ntiles, dim3(kFTW, kFTH), 0, st>>>(A);
+  VFS_LAUNCH_CHECK();
+}
+
+// upscale.cu:8-21, 46-61 for u, u-bar and warpUV (stereotgv.cu:497-510)
+__global__ void __launch_bounds__(kFTW* kFTH) k_upscale3(const __grid_constant__ UpArgs A) {
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  long long pos = ix + (long long)iy * P.s;
+  float x = ((float)ix + 0.5f) / (float)P.w;
+  float y = ((float)iy + 0.5f) / (float)P.h;
+  P.u_out[pos] = tex2D<float>(P.texU, x, y) * P.scale;
+  P.ubar_out[pos] = tex2D<float>(P.texUbar, x, y) * P.scale;
+  float2 v = tex2D<float2>(P.texWarp, x, y);
+  P.warp_out[pos] = make_float2(v.x * P.scale, v.y * P.scale);
+}
+
+void launch_upscale_batched(const UpArgs& A, cudaStream_t st) {
+  if (A.ntiles <= 0) return;
+  k_upscale3<<<A.ntiles, dim3(kFTW, kFTH), 0, st>>>(A);
+  VFS_LAUNCH_CHECK();
+}
+
+// downscale.cu:10-30 for I0 and I1 (stereotgv.cu:400-405)
+__global__ void __launch_bounds__(kFTW* kFTH) k_downscale2img(const __grid_constant__ DownArgs A) {
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  float dx = 1.0f / (float)P.w, dy = 1.0f / (float)P.h;
+  float x = ((float)ix + 0.5f) * dx, y = ((float)iy + 0.5f) * dy;
+  long long pos = ix + (long long)iy * P.s;
+  {
+    cudaTextureObject_t f = P.texI0;
+    float t1 = tex2D<float>(f, x - dx * 0.25f, y);
+    float t2 = tex2D<float>(f, x + dx * 0.25f, y);
+    float t3 = tex2D<float>(f, x, y - dy * 0.25f);
+    float t4 = tex2D<float>(f, x, y + dy * 0.25f);
+    P.I0[pos] = 0.25f * (t1 + t2 + t3 + t4);
+  }
+  {
+    cudaTextureObject_t f = P.texI1;
+    float t1 = tex2D<float>(f, x - dx * 0.25f, y);
+    float t2 = tex2D<float>(f, x + dx * 0.25f, y);
+    float t3 = tex2D<float>(f, x, y - dy * 0.25f);
+    float t4 = tex2D<float>(f, x, y + dy * 0.25f);
+    P.I1[pos] = 0.25f * (t1 + t2 + t3 + t4);
+  }
+}
+
+void launch_downscale_batched(const DownArgs& A, cudaStream_t st) {
+  if (A.ntiles <= 0) return;
+  k_downscale2img<<<A.ntiles, dim3(kFTW, kFTH), 0, st>>>(A);
+  VFS_LAUNCH_CHECK();
+}
+
+// Edge codes: masked form from the level's mask (neighbours outside the image are
+// off), plain form (mask == nullptr) flags the pixels inside the fixed circle.
+__global__ void k_edge_codes(const float* __restrict__ mask, uint8_t* code, int w, int h, int s) {
+  int ix = blockIdx.x * blockDim.x + threadIdx.x, iy = blockIdx.y * blockDim.y + threadIdx.y;
+  if (ix >= w || iy >= h) return;
+  long long pos = ix + (long long)iy * s;
+  uint8_t c = 0;
+  if (mask) {
+    if (mask[pos] != 0.0f) c |= kOn;
+    if (ix + 1 < w && mask[pos + 1] != 0.0f) c |= kR;
+    if (ix - 1 >= 0 && mask[pos - 1] != 0.0f) c |= kL;
+    if (iy + 1 < h && mask[pos + s] != 0.0f) c |= kD;
+    if (iy - 1 >= 0 && mask[pos - s] != 0.0f) c |= kU;
+  } else {
+    if (!outside_circle(ix, iy, w, h)) c |= kOn;
+  }
+  code[pos] = c;
+}
+
+void launch_edge_codes(const float* mask, uint8_t* code, int w, int h, int s, cudaStream_t st) {
+  k_edge_codes<<<dim3((w + 31) / 32, (h + 7) / 8), dim3(32, 8), 0, st>>>(mask, code, w, h, s);
+  VFS_LAUNCH_CHECK();
+}
+
+}  // namespace vfs

@@ -8,6 +8,7 @@
 #include "common.cuh"
 #include "kernels.cuh"
 #include "tgv_math.cuh"
+#include "tgv_pixel.cuh"
 
 namespace vfs {
 
@@ -22,15 +23,6 @@ __device__ __forceinline__ bool pixel(int& ix, int& iy, int w, int h) {
 // neighbour off); the reference reads out of bounds there.
 __device__ __forceinline__ float rd1(const float* b, long long k) { return k < 0 ? 0.0f : b[k]; }
 __device__ __forceinline__ float2 rd2(const float2* b, long long k) { return k < 0 ? make_float2(0.f, 0.f) : b[k]; }
-
-// updateDualVariables.cu:13-16: the plain kernels' fixed circular domain.
-__device__ __forceinline__ bool outside_circle(int ix, int iy, int w, int h) {
-  float desiredRadius = (float)w / 2.20f;
-  float halfWidth = (float)w / 2.0f;
-  float halfHeight = (float)h / 2.0f;
-  float radius = sqrtf((iy - halfHeight) * (iy - halfHeight) + (ix - halfWidth) * (ix - halfWidth));
-  return radius >= desiredRadius;
-}
 
 // ---------------------------------------------------------------------------
 __global__ void k_cv8u_to_gray(const uint8_t* src, float* dst, Geom g) {
@@ -192,9 +184,9 @@ __global__ void k_solve_eta(const float* __restrict__ mask, float alpha0, float 
   int pos = ix + iy * g.s;
   if (mask && mask[pos] == 0.0f) return;
   float a = A[pos], b = B[pos], c = C[pos];
-  etau[pos] = (a * a + b * b + 2 * c * c + (a + c) * (a + c) + (b + c) * (b + c)) * (alpha1 * alpha1);
-  etav1[pos] = (alpha1 * alpha1) * (b * b + c * c) + 4 * alpha0 * alpha0;
-  etav2[pos] = (alpha1 * alpha1) * (a * a + c * c) + 4 * alpha0 * alpha0;
+  etau[pos] = etau_math(a, b, c, alpha1);
+  etav1[pos] = etav1_math(b, c, alpha0, alpha1);
+  etav2[pos] = etav2_math(a, c, alpha0, alpha1);
 }
 
 __global__ void k_update_dual(DualArgs A, Geom g) {
@@ -220,34 +212,15 @@ __global__ void k_update_dual(DualArgs A, Geom g) {
   }
   float u_pos = A.u_[pos];
   float2 vp = A.v_[pos];
-  float u_x = useRight ? A.u_[right] - u_pos - vp.x : u_pos - rd1(A.u_, left) - vp.x;
-  float u_y = useDown ? A.u_[down] - u_pos - vp.y : u_pos - rd1(A.u_, up) - vp.y;
-  float a = A.a[pos], b = A.b[pos], c = A.c[pos];
-  float dtx = a * u_x + c * u_y;
-  float dty = c * u_x + b * u_y;
+  float u_xn = useRight ? A.u_[right] : rd1(A.u_, left);
+  float u_yn = useDown ? A.u_[down] : rd1(A.u_, up);
+  float2 v_xn = useRight ? A.v_[right] : rd2(A.v_, left);
+  float2 v_yn = useDown ? A.v_[down] : rd2(A.v_, up);
   float2 pp = A.p[pos];
-  float ppx = pp.x + (A.alpha1 * A.sigma / A.eta_p) * dtx;
-  float ppy = pp.y + (A.alpha1 * A.sigma / A.eta_p) * dty;
-  float rep = sqrtf(ppx * ppx + ppy * ppy);
-  if (rep < 1.0f) rep = 1.0f;
-  A.p[pos] = make_float2(ppx / rep, ppy / rep);
-  float2 vr = useRight ? A.v_[right] : make_float2(0.f, 0.f);
-  float2 vd = useDown ? A.v_[down] : make_float2(0.f, 0.f);
-  float2 vl = useRight ? make_float2(0.f, 0.f) : rd2(A.v_, left);
-  float2 vu = useDown ? make_float2(0.f, 0.f) : rd2(A.v_, up);
-  float gvx = useRight ? vr.x - vp.x : vp.x - vl.x;
-  float gvy = useDown ? vd.y - vp.y : vp.y - vu.y;
-  float gvz = useDown ? vd.x - vp.x : vp.x - vu.x;
-  float gvw = useRight ? vr.y - vp.y : vp.y - vl.y;
-  float ase = A.alpha0 * A.sigma / A.eta_q;
   float4 qq = A.q[pos];
-  float qx = qq.x + ase * gvx;
-  float qy = qq.y + ase * gvy;
-  float qz = qq.z + ase * gvz;
-  float qw = qq.w + ase * gvw;
-  float reproj = sqrtf(qx * qx + qy * qy + qz * qz + qw * qw);
-  if (reproj < 1.0f) reproj = 1.0f;
-  A.q[pos] = make_float4(qx / reproj, qy / reproj, qz / reproj, qw / reproj);
+  dual_math(useRight, useDown, u_pos, u_xn, u_yn, vp, v_xn, v_yn, A.a[pos], A.b[pos], A.c[pos], A.sp, A.sq, pp, qq);
+  A.p[pos] = pp;
+  A.q[pos] = qq;
 }
 
 __global__ void k_solve_tp(const float* __restrict__ mask, const float* __restrict__ A, const float* __restrict__ B,
@@ -256,9 +229,7 @@ __global__ void k_solve_tp(const float* __restrict__ mask, const float* __restri
   if (!pixel(ix, iy, g.w, g.h)) return;
   int pos = ix + iy * g.s;
   if (mask && mask[pos] == 0.0f) return;
-  float2 pp = p[pos];
-  float a = A[pos], b = B[pos], c = C[pos];
-  Tp[pos] = make_float2(a * pp.x + c * pp.y, c * pp.x + b * pp.y);
+  Tp[pos] = tp_math(A[pos], B[pos], C[pos], p[pos]);
 }
 
 __global__ void k_thresholding(ThreshArgs A, Geom g) {
@@ -291,26 +262,7 @@ __global__ void k_thresholding(ThreshArgs A, Geom g) {
     else if (iy == g.h - 1) dym = -rd2(A.Tp, up).y;
     else dym = A.Tp[pos].y;
   }
-  float div_p = dxm + dym;
-  float eu = A.etau[pos];
-  float tau_eta_u = (eu == 0.0f) ? A.tau : A.tau / eu;
-  float uhat = A.u_[pos] + tau_eta_u * div_p;
-  float upos = A.u[pos];
-  float dun = uhat - upos;
-  float Ius = A.Iu[pos];
-  float rho = Ius * dun + A.Iz[pos];
-  float upper = A.lambda * tau_eta_u * (Ius * Ius);
-  float lower = -A.lambda * tau_eta_u * (Ius * Ius);
-  float d = 0.0f;
-  if ((rho <= upper) && (rho >= lower)) {
-    if (Ius == 0.0f) d = dun;
-    else d = dun - rho / Ius;
-  } else if (rho < lower) {
-    d = dun + A.lambda * tau_eta_u * Ius;
-  } else if (rho > upper) {
-    d = dun - A.lambda * tau_eta_u * Ius;
-  }
-  A.us[pos] = upos + d;
+  A.us[pos] = threshold_math(dxm, dym, A.etau[pos], A.tau, A.u_[pos], A.u[pos], A.Iu[pos], A.Iz[pos], A.lambda);
 }
 
 __global__ void k_update_primal(PrimalArgs A, Geom g) {
@@ -341,65 +293,24 @@ __global__ void k_update_primal(PrimalArgs A, Geom g) {
     hasU = (iy - 1) >= 0;
   }
   float4 qc = A.q[pos];
-  float qcx = zR ? 0.0f : qc.x, qcw = zR ? 0.0f : qc.w;
-  float qcy = zD ? 0.0f : qc.y, qcz = zD ? 0.0f : qc.z;
+  if (zR) qc.x = qc.w = 0.0f;
+  if (zD) qc.y = qc.z = 0.0f;
   float4 ql = hasL ? A.q[left] : make_float4(0.f, 0.f, 0.f, 0.f);
   float4 qu = hasU ? A.q[up] : make_float4(0.f, 0.f, 0.f, 0.f);
-  float dqx = (qcx - ql.x) + (qcz - qu.z);
-  float dqy = (qcw - ql.w) + (qcy - qu.y);
-  float2 pp = A.p[pos];
-  float a = A.a[pos], b = A.b[pos], c = A.c[pos];
-  float dtx = a * pp.x + c * pp.y;
-  float dty = c * pp.x + b * pp.y;
-  float ev1 = A.etav1[pos], ev2 = A.etav2[pos];
-  float2 vb = A.v_[pos];
-  float vx, vy;
-  if (ev1 != 0.0f) vx = vb.x + (A.tau / ev1) * (A.alpha1 * dtx + A.alpha0 * dqx);
-  else vx = vb.x + (A.tau) * (A.alpha1 * dtx + A.alpha0 * dqx);
-  if (ev2 != 0.0f) {
-    vy = vb.y + (A.tau / ev2) * (A.alpha1 * dty + A.alpha0 * dqy);
-  } else {  // updatePrimalVariables.cu:103-105 writes .x again; .y keeps the previous value
-    vx = vb.x + (A.tau) * (A.alpha1 * dtx + A.alpha0 * dqx);
-    vy = vb.y;
-  }
-  A.v[pos] = make_float2(vx, vy);
-  float up_ = A.u[pos];
-  A.u_s[pos] = up_ + A.mu * (up_ - A.u_[pos]);
-  A.v_s[pos] = make_float2(vx + A.mu * (vx - vb.x), vy + A.mu * (vy - vb.y));
+  float us_;
+  float2 vs, vo;
+  primal_math(qc, ql, qu, A.p[pos], A.a[pos], A.b[pos], A.c[pos], A.etav1[pos], A.etav2[pos], A.tau, A.alpha0,
+              A.alpha1, A.mu, A.v_[pos], A.u[pos], A.u_[pos], us_, vs, vo);
+  A.v[pos] = vo;
+  A.u_s[pos] = us_;
+  A.v_s[pos] = vs;
 }
 
-// 5x5 median with the reference's border rule: a tap outside the image in exactly
-// one direction is clamped to the edge, a tap outside in both directions (corner)
-// is 0.  The 13th smallest of the 25 taps equals the reference's partial
-// selection sort result (medianFilter.cu:306-318).
+// medianFilter.cu:264-319
 __global__ void k_median5(const float* __restrict__ in, float* out, Geom g) {
   int ix, iy;
   if (!pixel(ix, iy, g.w, g.h)) return;
-  float m[25];
-#pragma unroll
-  for (int j = 0; j < 5; j++) {
-#pragma unroll
-    for (int i = 0; i < 5; i++) {
-      int col = ix + i - 2, row = iy + j - 2;
-      bool cin = col >= 0 && col < g.w, rin = row >= 0 && row < g.h;
-      float v = 0.0f;
-      if (cin || rin) {
-        int cc = min(max(col, 0), g.w - 1), rr = min(max(row, 0), g.h - 1);
-        v = in[cc + rr * g.s];
-      }
-      m[j * 5 + i] = v;
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < 13; j++) {
-#pragma unroll
-    for (int i = j + 1; i < 25; i++) {
-      float lo = fminf(m[j], m[i]), hi = fmaxf(m[j], m[i]);
-      m[j] = lo;
-      m[i] = hi;
-    }
-  }
-  out[ix + iy * g.s] = m[12];
+  out[ix + iy * g.s] = median5_at(in, ix, iy, g.w, g.h, g.s);
 }
 
 __global__ void k_warp_epilogue(float* u, const float* __restrict__ u_last, float* du, float* u_,
@@ -598,7 +509,10 @@ void launch_solve_eta(const float* mask, float alpha0, float alpha1, const float
   k_solve_eta<<<L2D(g)>>>(mask, alpha0, alpha1, a, b, c, etau, etav1, etav2, g);
   VFS_LAUNCH_CHECK();
 }
-void launch_update_dual(const DualArgs& A, Geom g, cudaStream_t st) {
+void launch_update_dual(const DualArgs& A0, Geom g, cudaStream_t st) {
+  DualArgs A = A0;
+  A.sp = A.alpha1 * A.sigma / A.eta_p;  // updateDualVariables.cu:174-176, uniform per launch
+  A.sq = A.alpha0 * A.sigma / A.eta_q;  // updateDualVariables.cu:217
   k_update_dual<<<L2D(g)>>>(A, g);
   VFS_LAUNCH_CHECK();
 }

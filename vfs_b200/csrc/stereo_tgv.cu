@@ -9,12 +9,91 @@ namespace vfs {
 
 StereoTgvImpl::StereoTgvImpl(int bw, int bh, int sa) : blockWidth(bw), blockHeight(bh), strideAlignment(sa) {}
 
-StereoTgvImpl::~StereoTgvImpl() { release(); }
+StereoTgvImpl::~StereoTgvImpl() {
+  release();
+  for (auto e : evpool_) cudaEventDestroy(e);
+  if (own_stream_) cudaStreamDestroy(own_stream_);
+}
+
+cudaStream_t StereoTgvImpl::own_stream() {
+  if (!own_stream_) VFS_CUDA(cudaStreamCreateWithFlags(&own_stream_, cudaStreamNonBlocking));
+  return own_stream_;
+}
+
+std::atomic<long long>& launch_counter() {
+  static std::atomic<long long> n{0};
+  return n;
+}
+
+cudaEvent_t StereoTgvImpl::profEvent() {
+  if (capture_events) {
+    cudaEvent_t e;
+    VFS_CUDA(cudaEventCreate(&e));
+    capture_events->push_back(e);
+    return e;
+  }
+  if (evused_ == evpool_.size()) {
+    cudaEvent_t e;
+    VFS_CUDA(cudaEventCreate(&e));
+    evpool_.push_back(e);
+  }
+  return evpool_[evused_++];
+}
+
+static void record(cudaEvent_t e, cudaStream_t st, bool external) {
+  if (external) VFS_CUDA(cudaEventRecordWithFlags(e, st, cudaEventRecordExternal));
+  else VFS_CUDA(cudaEventRecord(e, st));
+}
+
+void StereoTgvImpl::profBegin(int tag, int level, int iters) {
+  profBeginPx(tag, (long long)pW[level] * pH[level], iters);
+}
+
+void StereoTgvImpl::profBeginPx(int tag, long long px, int iters) {
+  if (!profiling) return;
+  ProfRec r{tag, 0, px, iters, profEvent(), profEvent()};
+  record(r.a, stream_, capture_events != nullptr);
+  prof_.push_back(r);
+}
+
+void StereoTgvImpl::profEnd() {
+  if (!profiling || prof_.empty()) return;
+  record(prof_.back().b, stream_, capture_events != nullptr);
+}
+
+void StereoTgvImpl::profReset() {
+  prof_.clear();
+  evused_ = 0;
+}
+
+void StereoTgvImpl::profRead(int tag, long long* count, double* total_ms, double* pixel_iters) {
+  VFS_CUDA(cudaStreamSynchronize(stream_));
+  long long n = 0;
+  double t = 0, pi = 0;
+  for (auto& r : prof_) {
+    if (r.tag != tag) continue;
+    float ms = 0;
+    VFS_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+    n++;
+    t += ms;
+    pi += (double)r.px * r.iters;
+  }
+  if (count) *count = n;
+  if (total_ms) *total_ms = t;
+  if (pixel_iters) *pixel_iters = pi;
+}
 
 void StereoTgvImpl::release() {
+  engine.clear();
   tex.clear();
   if (pool_) cudaFree(pool_);
   pool_ = nullptr;
+  if (fpool_) cudaFree(fpool_);
+  fpool_ = nullptr;
+  f_p = f_q = f_vh = f_vhs = nullptr;
+  code_masked.clear();
+  code_plain.clear();
+  codes_valid = false;
   pool_bytes_ = pool_used_ = 0;
   initialized_ = false;
 }
@@ -39,6 +118,9 @@ void StereoTgvImpl::initialize(const SolverParams& p) {
   if (strideAlignment <= 0 || blockWidth <= 0 || blockHeight <= 0)
     throw ArgError{"initialize: invalid block or stride alignment"};
   release();
+  if (!stream_) stream_ = own_stream();
+  static std::atomic<uint64_t> gen{0};
+  generation = ++gen;
   P = p;
   width = p.width;
   height = p.height;
@@ -63,6 +145,8 @@ void StereoTgvImpl::initialize(const SolverParams& p) {
     ns = align_up(nw, strideAlignment);
   }
   full_ = (size_t)stride * height;
+  if (full_ * 8 >= ((size_t)1 << 31))
+    throw ArgError{"initialize: image too large (row pitch x height x 8 must stay below 2^31)"};
   size_t f = full_ * sizeof(float);
   // pool: pyramid (5 planes/level: I0, I1, mask, tv x2); full-resolution planes:
   // 18 float, 10 float2, 1 float4, 2 float3, 1 four-plane staging; u8 and uchar3
@@ -158,6 +242,7 @@ void StereoTgvImpl::copyMaskToDevice(const float* mask) {
   VFS_CUDA(cudaMemcpy2DAsync(pMask[0], (size_t)stride * sizeof(float), mask, row, row, height, cudaMemcpyHostToDevice,
                              stream_));
   for (int l = 1; l < P.nLevels; l++) launch_downscale_nearest(t1(pMask[l - 1], l - 1, false), pMask[l], geom(l), stream_);
+  codes_valid = false;
   VFS_CUDA(cudaStreamSynchronize(stream_));
 }
 
@@ -197,7 +282,47 @@ void StereoTgvImpl::copyImagesU8C3(const uint8_t* i0, const uint8_t* i1) {
 
 void StereoTgvImpl::solve(bool masked) {
   if (!initialized_) throw ArgError{"solve before initialize"};
-  solveReference(masked);
+  if (path == SolvePath::kFused) {
+    std::vector<StereoTgvImpl*> one{this};
+    engine.solve(one, masked, half_storage, stream_);
+  } else {
+    solveReference(masked);
+  }
+}
+
+// Fused-path buffers: p and q in two planes each (float: 8 + 16 bytes per pixel per
+// plane; half: 4 + 8), half v-bar ping-pong pair (4 + 4), and per-level edge codes.
+void StereoTgvImpl::ensureFused() {
+  if (fpool_) return;
+  size_t n = full_;
+  size_t bytes = n * 2 * 8 + n * 2 * 16 + n * 4 * 2 + 8 * 512;
+  for (int l = 0; l < levels(); l++) bytes += 2 * ((size_t)pS[l] * pH[l] + 512);
+  cudaError_t e = cudaMalloc(&fpool_, bytes);
+  if (e != cudaSuccess) {
+    fpool_ = nullptr;
+    (void)cudaGetLastError();
+    throw CudaError{e, "cudaMalloc(fused buffers)", __FILE__, __LINE__};
+  }
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    off = (off + 511) & ~(size_t)511;
+    char* p = fpool_ + off;
+    off += b;
+    return p;
+  };
+  f_p = take(n * 2 * 8);
+  f_q = take(n * 2 * 16);
+  f_vh = take(n * 4);
+  f_vhs = take(n * 4);
+  code_masked.assign(levels(), nullptr);
+  code_plain.assign(levels(), nullptr);
+  for (int l = 0; l < levels(); l++) {
+    code_masked[l] = (uint8_t*)take((size_t)pS[l] * pH[l]);
+    code_plain[l] = (uint8_t*)take((size_t)pS[l] * pH[l]);
+  }
+  VFS_CUDA(cudaMemsetAsync(fpool_, 0, bytes, stream_));
+  for (int l = 0; l < levels(); l++) launch_edge_codes(nullptr, code_plain[l], pW[l], pH[l], pS[l], stream_);
+  codes_valid = false;
 }
 
 // stereotgv.cu:389-515 (masked) and 256-387 (plain).  Pointer swaps are the
@@ -242,6 +367,7 @@ void StereoTgvImpl::solveReference(bool masked) {
         float mu;
         if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P.timestep_lambda);
         else mu = 1;
+        profBegin(kProfInner, level, 1);
         DualArgs da{mk, d_u_, d_v_, d_a, d_b, d_c, d_p, d_q, P.alpha0, P.alpha1, sigma, eta_p, eta_q};
         launch_update_dual(da, g, st);
         launch_solve_tp(mk, d_a, d_b, d_c, d_p, d_Tp, g, st);
@@ -251,6 +377,7 @@ void StereoTgvImpl::solveReference(bool masked) {
         PrimalArgs pa{mk, d_u_, d_v_, d_p, d_q, d_a, d_b, d_c, d_etav1, d_etav2, d_u, d_v, d_u_s, d_v_s,
                       tau, P.alpha0, P.alpha1, mu};
         launch_update_primal(pa, g, st);
+        profEnd();
         std::swap(d_u_, d_u_s);
         std::swap(d_v_, d_v_s);
         sigma = sigma / mu;

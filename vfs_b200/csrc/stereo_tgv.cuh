@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "fused.cuh"
 #include "kernels.cuh"
 
 namespace vfs {
@@ -28,13 +29,45 @@ enum class SolvePath {
   kFused = 1,      // fused kernels with temporal blocking
 };
 
+class StereoTgvImpl;
+
+// physical buffers that the solve's pointer swaps move between roles
+struct PairPtrs {
+  float *pI1_0, *i1cal, *u, *us, *u_, *u_s;
+  float2 *v_, *v_s, *warpUV, *warpUVs;
+  void *vh, *vhs;
+};
+
+// Runs the fused path for a set of pairs, optionally through a cache of captured
+// CUDA graphs (one per batch composition and pointer state).
+class FusedEngine {
+ public:
+  bool use_graph = true;
+  ~FusedEngine();
+  void clear();
+  void solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st);
+  // allocate fused buffers and refresh edge codes, each on the pair's own stream
+  static void prepare(std::vector<StereoTgvImpl*>& pairs, bool masked);
+  size_t graphs() const { return cache_.size(); }
+
+ private:
+  struct Entry {
+    cudaGraphExec_t exec = nullptr;
+    std::vector<PairPtrs> after;
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> events;
+  };
+  std::map<std::vector<uintptr_t>, Entry> cache_;
+};
+
 class StereoTgvImpl {
  public:
   StereoTgvImpl(int blockWidth, int blockHeight, int strideAlignment);
   ~StereoTgvImpl();
 
   void initialize(const SolverParams& p);
-  void setStream(cudaStream_t st) { stream_ = st; }
+  // a handle runs on its own non-blocking stream unless the caller sets one
+  void setStream(cudaStream_t st) { stream_ = st ? st : own_stream(); }
   cudaStream_t stream() const { return stream_; }
   bool initialized() const { return initialized_; }
 
@@ -57,7 +90,26 @@ class StereoTgvImpl {
   int width = 0, height = 0, stride = 0;
   std::vector<int> pW, pH, pS;
   SolvePath path = SolvePath::kReference;
+  bool half_storage = false;  // fused path: p, q, v-bar stored as half
   std::string last_error;
+
+  // ---- fused-path state (allocated on first use) ------------------------------
+  // p and q: two planes each (read one, write the other per iteration), float or
+  // half; v-bar in half storage: its own ping-pong pair (float storage uses d_v_ /
+  // d_v_s); edge codes per level for the masked and the plain form.
+  void ensureFused();
+  void* f_p = nullptr;
+  void* f_q = nullptr;
+  void* f_vh = nullptr;  // current half v-bar
+  void* f_vhs = nullptr; // other half v-bar
+  std::vector<uint8_t*> code_masked, code_plain;
+  bool codes_valid = false;
+  int f_parity = 0;      // which p / q plane holds the latest values
+  int levels() const { return (int)pW.size(); }
+  Geom geomAt(int level) const { return Geom{pW[level], pH[level], pS[level]}; }
+  cudaTextureObject_t tex1(const float* p, int level, bool linear = true) { return t1(p, level, linear); }
+  cudaTextureObject_t tex2(const float2* p, int level) { return t2(p, level); }
+  size_t fullElems() const { return full_; }
 
   // ---- device state (names follow stereotgv.h:48-96) ------------------------
   std::vector<float*> pI0, pI1, pMask;
@@ -80,6 +132,18 @@ class StereoTgvImpl {
   size_t pool_bytes() const { return pool_bytes_; }
   TexCache tex;
 
+  // ---- opt-in event timing of launch groups (bench / profiling) -----------
+  bool profiling = false;
+  void profReset();
+  // Sum over records of `tag` (kProf*): count, total milliseconds, pixel-iterations.
+  void profRead(int tag, long long* count, double* total_ms, double* pixel_iters);
+  std::vector<ProfRec> profRecords() const { return prof_; }
+  void setProfRecords(const std::vector<ProfRec>& r) { prof_ = r; }
+  // while a graph is captured, profiling events are created here (owned by the graph)
+  std::vector<cudaEvent_t>* capture_events = nullptr;
+  FusedEngine engine;  // single-pair fused solves
+  uint64_t generation = 0;  // incremented by every initialize (invalidates captured graphs)
+
  private:
   void release();
   float* alloc(size_t bytes);
@@ -92,8 +156,22 @@ class StereoTgvImpl {
   }
   void solveReference(bool masked);
 
+ public:
+  cudaEvent_t profEvent();
+  void profBegin(int tag, int level, int iters);
+  void profBeginPx(int tag, long long px, int iters);
+  void profEnd();
+
+ private:
+  std::vector<ProfRec> prof_;
+  std::vector<cudaEvent_t> evpool_;
+  size_t evused_ = 0;
+
+  cudaStream_t own_stream();
   bool initialized_ = false;
+  cudaStream_t own_stream_ = nullptr;
   cudaStream_t stream_ = 0;
+  char* fpool_ = nullptr;
   char* pool_ = nullptr;
   size_t pool_bytes_ = 0, pool_used_ = 0;
   size_t full_ = 0;  // elements of a full-resolution pitched plane

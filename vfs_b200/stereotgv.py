@@ -13,9 +13,12 @@ from typing import Optional, Tuple
 
 import numpy as np
 
-from ._native import VfsError, check, lib
+from ._native import VfsError, check, check_batch, lib
 
-__all__ = ["StereoTgv", "VfsError"]
+__all__ = ["StereoTgv", "StereoBatch", "VfsError"]
+
+PATH_REFERENCE = 0
+PATH_FUSED = 1
 
 
 def _ptr(a: np.ndarray):
@@ -70,6 +73,15 @@ class StereoTgv:
 
     def synchronize(self) -> None:
         check(self._h, self._L.vfs_synchronize(self._h))
+
+    def set_solve_path(self, fused: bool, half_storage: bool = False) -> None:
+        """Select the drop-in path (one kernel per reference kernel) or the fused path
+        (optionally with p, q, v-bar stored as half)."""
+        check(self._h, self._L.vfs_set_solve_path(self._h, PATH_FUSED if fused else PATH_REFERENCE,
+                                                  int(half_storage)))
+
+    def set_graph(self, on: bool) -> None:
+        check(self._h, self._L.vfs_set_graph(self._h, int(on)))
 
     # ---- reference methods -------------------------------------------------
     def initialize(self, width, height, beta, gamma, alpha0, alpha1, timestep_lambda, lambda_,
@@ -177,6 +189,23 @@ class StereoTgv:
         check(self._h, self._L.vfs_copy_disparity_vis_to_host(self._h, _ptr(out), flowScale))
         return out
 
+    # ---- measurement hooks ---------------------------------------------------
+    @staticmethod
+    def launch_count() -> int:
+        return int(lib().vfs_launch_count())
+
+    def profile(self, on: bool) -> None:
+        check(self._h, self._L.vfs_profile_enable(self._h, int(on)))
+
+    def profile_reset(self) -> None:
+        check(self._h, self._L.vfs_profile_reset(self._h))
+
+    def profile_read(self, kind: int):
+        """(launches, total_ms, pixel_iterations) of a timed launch group kind."""
+        n, ms, pi = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+        check(self._h, self._L.vfs_profile_read(self._h, kind, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(pi)))
+        return n.value, ms.value, pi.value
+
     def debug_buffer(self, name: str, comps: int = 1) -> np.ndarray:
         out = np.empty((self.height, self.width, comps), np.float32)
         check(self._h, self._L.vfs_debug_get_buffer(self._h, name.encode(), comps, _ptr(out)))
@@ -186,3 +215,56 @@ class StereoTgv:
     def _check_shape(a: np.ndarray, shape, what: str) -> None:
         if tuple(a.shape) != tuple(shape):
             raise VfsError(-1, f"{what}: expected shape {tuple(shape)}, got {tuple(a.shape)}")
+
+
+class StereoBatch:
+    """Several :class:`StereoTgv` pairs solved together by the fused path (one launch per step
+    and level for all pairs, replayed as a CUDA graph)."""
+
+    def __init__(self, half_storage: bool = False, stream=None):
+        self._L = lib()
+        h = ctypes.c_void_p()
+        st = self._L.vfs_batch_create(ctypes.byref(h))
+        if st != 0:
+            raise VfsError(st, "vfs_batch_create failed")
+        self._h = h
+        self.members = []
+        self.set_storage(half_storage)
+        if stream is not None:
+            self.set_stream(stream)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            try:
+                self._L.vfs_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def set_stream(self, stream) -> None:
+        """Run the batched work on this stream; members keep their own streams and are
+        ordered before / after each batch solve with events."""
+        raw = getattr(stream, "cuda_stream", stream)
+        self._stream = stream
+        check_batch(self._h, self._L.vfs_batch_set_stream(self._h, ctypes.c_void_p(int(raw) if raw else 0)))
+
+    def set_storage(self, half_storage: bool) -> None:
+        check_batch(self._h, self._L.vfs_batch_set_storage(self._h, int(half_storage)))
+
+    def set_graph(self, on: bool) -> None:
+        check_batch(self._h, self._L.vfs_batch_set_graph(self._h, int(on)))
+
+    def add(self, solver: "StereoTgv") -> None:
+        check_batch(self._h, self._L.vfs_batch_add(self._h, solver.handle))
+        self.members.append(solver)
+
+    def clear(self) -> None:
+        check_batch(self._h, self._L.vfs_batch_clear(self._h))
+        self.members = []
+
+    def solve(self, masked: bool = True) -> None:
+        check_batch(self._h, self._L.vfs_batch_solve(self._h, int(masked)))
+
+    def __len__(self):
+        return len(self.members)
