@@ -183,7 +183,14 @@ void launch_edge_codes(const float* mask, uint8_t* code, int w, int h, int s, cu
 inline int tiles_x_of(int w) { return (w + kFTW - 1) / kFTW; }
 inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFTH); }
 // the iteration kernel's tiles: 31 x kIterTH pixels (a 32 x (kIterTH + 1) block with halo)
-constexpr int kIterTH = 8;
+#ifndef VFS_ITER_TH
+#define VFS_ITER_TH 8
+#endif
+#ifndef VFS_ITER_MINB
+#define VFS_ITER_MINB 7
+#endif
+constexpr int kIterTH = VFS_ITER_TH;
+constexpr int kIterMinBlocks = VFS_ITER_MINB;  // __launch_bounds__ minimum resident blocks per SM
 inline int iter_tiles_x_of(int w) { return (w + 30) / 31; }
 inline int iter_tiles_of(int w, int h) { return iter_tiles_x_of(w) * ((h + kIterTH - 1) / kIterTH); }
 

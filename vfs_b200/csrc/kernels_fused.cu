@@ -84,7 +84,8 @@ struct FusedIter {
 // finish the threshold and primal steps with the west / north values from shared
 // memory.
 template <bool MASKED, class ST, int TH>
-__global__ void __launch_bounds__(32 * (TH + 1)) k_fused_iter(const __grid_constant__ IterArgs A, int parity) {
+__global__ void __launch_bounds__(32 * (TH + 1), kIterMinBlocks) k_fused_iter(const __grid_constant__ IterArgs A,
+                                                                              int parity) {
   typedef FusedIter<MASKED, ST> F;
   typedef typename F::T2 T2;
   typedef typename F::T4 T4;
