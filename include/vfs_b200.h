@@ -133,6 +133,12 @@ int vfs_batch_set_storage(vfs_batch* b, int half_storage);
 int vfs_batch_set_graph(vfs_batch* b, int use_graph);
 int vfs_batch_solve(vfs_batch* b, int masked);
 
+/* Histogram equalisation of n 8-bit pixels in device memory (d_dst may equal d_src), as
+ * cv::equalizeHist, which the reference's SolveStereo applies to both images on the host
+ * (dllhook/vfs.cpp:36-37).  Stream-ordered on cuda_stream; its 1280 bytes of scratch are
+ * allocated and freed on that stream (cudaMallocAsync / cudaFreeAsync). */
+int vfs_equalize_hist_u8(const uint8_t* d_src, uint8_t* d_dst, size_t n, void* cuda_stream);
+
 /* Measurement hooks (no counterpart in the reference).  vfs_launch_count() is the number
  * of kernels this library has launched in the process.  With profiling on, each group of
  * inner primal-dual kernels (one iteration in the drop-in path, one fused launch of several

@@ -28,7 +28,7 @@ def params(beta=10.0, gamma=0.8, alpha0=17.0, alpha1=1.2, tsl=1.0, lam=5.0, n_le
 
 def run_gpu(i0, i1, mask, tv, cv, p, masked=True, frames=1, solver=None):
     from vfs_b200.stereotgv import StereoTgv
-    h, w = i0.shape
+    h, w = i0.shape[:2]
     s = solver or StereoTgv()
     s.limitRange = p["limit_range"]
     s.initialize(w, h, p["beta"], p["gamma"], p["alpha0"], p["alpha1"], p["tsl"], p["lam"], p["n_levels"],

@@ -337,6 +337,31 @@ int vfs_batch_solve(vfs_batch* b, int masked) {
   });
 }
 
+int vfs_equalize_hist_u8(const uint8_t* d_src, uint8_t* d_dst, size_t n, void* cuda_stream) {
+  if (n == 0) return VFS_OK;
+  if (!d_src || !d_dst) return VFS_ERR_ARG;
+  if (n > 0xFFFFFFFFull) return VFS_ERR_ARG;  // 32-bit histogram counters
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  void* scratch = nullptr;
+  if (cudaMallocAsync(&scratch, 256 * sizeof(unsigned int) + 256, st) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return VFS_ERR_NOMEM;
+  }
+  int rc = VFS_OK;
+  try {
+    vfs::launch_equalize_hist(d_src, d_dst, n, (unsigned int*)scratch, (uint8_t*)scratch + 256 * sizeof(unsigned int),
+                              st);
+  } catch (const vfs::CudaError&) {
+    (void)cudaGetLastError();
+    rc = VFS_ERR_CUDA;
+  }
+  if (cudaFreeAsync(scratch, st) != cudaSuccess) {
+    (void)cudaGetLastError();
+    rc = VFS_ERR_CUDA;
+  }
+  return rc;
+}
+
 long long vfs_launch_count(void) { return vfs::launch_counter().load(); }
 
 int vfs_profile_enable(vfs_stereo* s, int on) {
