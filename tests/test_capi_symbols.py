@@ -18,6 +18,8 @@ def declared_functions():
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         src = re.sub(r"//[^\n]*", "", src)
         src = "\n".join(l for l in src.splitlines() if not l.lstrip().startswith("#"))
+        if 'extern "C" {' not in src:
+            continue  # C++ headers (stereotgv.h) declare no exported symbols
         body = src.split('extern "C" {', 1)[-1]
         for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", body):
             name = m.group(1)
@@ -45,3 +47,32 @@ def test_status_strings_without_gpu():
     assert lib.vfs_status_string(-1) == b"invalid argument"
     lib.vfs_version.restype = ctypes.c_int
     assert lib.vfs_version() >= 100
+
+
+def test_cpp_dropin_header_compiles_links_and_runs_without_gpu(tmp_path):
+    """include/stereotgv.h: a program written against the reference class compiles, links
+    against the library and, without a GPU, gets an error status instead of exiting."""
+    import subprocess
+    build()
+    src = tmp_path / "t.cpp"
+    src.write_text(r"""
+#include "stereotgv.h"
+#include <cstdio>
+int main() {
+  StereoTgv s;                      // reference constructor
+  s.limitRange = 0.1f;              // reference public field
+  int st = s.initialize(64, 48, 10.0f, 0.8f, 17.0f, 1.2f, 1.0f, 5.0f, 2, 2.0f, 1, 1);
+  std::printf("%d %s\n", st, vfs_status_string(st));
+  return 0;
+}
+""")
+    exe = tmp_path / "t"
+    inc = os.path.join(ROOT, "include")
+    libdir = os.path.dirname(LIB)
+    r = subprocess.run(["g++", "-std=c++17", f"-I{inc}", str(src), "-o", str(exe), f"-L{libdir}", "-lvfs_b200",
+                        f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, r.stderr
+    code = int(r.stdout.split()[0])
+    assert code in (0, -2), r.stdout  # 0 on a GPU machine, VFS_ERR_CUDA without a device
