@@ -139,6 +139,23 @@ int vfs_batch_solve(vfs_batch* b, int masked);
  * allocated and freed on that stream (cudaMallocAsync / cudaFreeAsync). */
 int vfs_equalize_hist_u8(const uint8_t* d_src, uint8_t* d_dst, size_t n, void* cuda_stream);
 
+/* Histogram equalisation that allocates nothing (no counterpart in the reference).
+ * For callers that cannot allocate device memory at the point of the call: code recorded
+ * into a CUDA graph or running inside a stream capture, where an allocation would become
+ * part of the capture or be refused; real-time camera threads, where cudaMalloc / cudaFree
+ * can stall on device-wide synchronisation; and hosts whose device memory is already
+ * reserved by another allocator.  It equalises `count` images of n pixels each, stored back
+ * to back at d_src (results at d_dst, which may equal d_src), like vfs_equalize_hist_u8.
+ * Limits: count <= VFS_NOALLOC_MAX_IMAGES (16) and n <= 2^32 - 1; larger requests return
+ * VFS_ERR_ARG with a message in vfs_last_error(NULL).  The scratch is a 20 KiB array that
+ * each GPU loading the library keeps until exit, shared by every call on that GPU: calls
+ * whose work overlaps on the GPU (different streams, or host threads without ordering)
+ * race on it, so order them on one stream.  The first call on a device resolves the
+ * array's device address; make that first call before any stream capture. */
+#define VFS_NOALLOC_MAX_IMAGES 16
+int vfs_equalize_hist_u8_noalloc(const uint8_t* d_src, uint8_t* d_dst, size_t n, int count,
+                                 void* cuda_stream);
+
 /* Measurement hooks (no counterpart in the reference).  vfs_launch_count() is the number
  * of kernels this library has launched in the process.  With profiling on, each group of
  * inner primal-dual kernels (one iteration in the drop-in path, one fused launch of several

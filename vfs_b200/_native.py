@@ -74,6 +74,7 @@ SIGNATURES = {
     "vfs_batch_set_graph": [_vp, _i],
     "vfs_batch_solve": [_vp, _i],
     "vfs_equalize_hist_u8": [_vp, _vp, _sz, _vp],
+    "vfs_equalize_hist_u8_noalloc": [_vp, _vp, _sz, _i, _vp],
     "vfs_launch_count": [],
     "vfs_profile_enable": [_vp, _i],
     "vfs_profile_reset": [_vp],

@@ -69,6 +69,11 @@ int guarded(H* s, F&& f) {
 
 }  // namespace
 
+namespace vfs {
+// message of the last failure of a call that has no handle (read with vfs_last_error(NULL))
+void set_global_error(const char* msg) { g_create_error = msg; }
+}  // namespace vfs
+
 extern "C" {
 
 const char* vfs_status_string(int st) {

@@ -6,6 +6,9 @@
 //   else scale = 255 / (total - hist[i]); lut[i] = 0;
 //        lut[j] = round_half_even(scale * sum_{i<k<=j} hist[k]) for j > i,
 //        saturated to 0..255.
+#include <mutex>
+
+#include "../../include/vfs_b200.h"
 #include "common.cuh"
 #include "hist.cuh"
 
@@ -83,3 +86,78 @@ void launch_equalize_hist(const uint8_t* src, uint8_t* dst, size_t n, unsigned i
 }
 
 }  // namespace vfs
+
+// ---------------------------------------------------------------------------
+// Equalisation without any allocation (vfs_equalize_hist_u8_noalloc).
+//
+// Its scratch -- one 256-bin histogram and one 256-byte LUT per image -- lives in this
+// file-scope device array, which every GPU that loads the library holds until the process
+// exits.  Host code cannot use the array's name as a device address (on the host it is
+// only a stand-in), so the first call on each device resolves the address with
+// cudaGetSymbolAddress while that device is current and keeps it for later calls.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kSlotBytes = 256 * sizeof(unsigned int) + 256;  // histogram + LUT of one image
+static __device__ __align__(256) unsigned char g_noalloc_scratch[VFS_NOALLOC_MAX_IMAGES * kSlotBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+}  // namespace
+
+namespace vfs {
+void set_global_error(const char* msg);
+}
+
+extern "C" int vfs_equalize_hist_u8_noalloc(const uint8_t* d_src, uint8_t* d_dst, size_t n, int count,
+                                            void* cuda_stream) {
+  if (count < 0 || count > VFS_NOALLOC_MAX_IMAGES) {
+    vfs::set_global_error("vfs_equalize_hist_u8_noalloc: count exceeds VFS_NOALLOC_MAX_IMAGES (16)");
+    return VFS_ERR_ARG;
+  }
+  if (n > 0xFFFFFFFFull) {
+    vfs::set_global_error("vfs_equalize_hist_u8_noalloc: more than 2^32 - 1 pixels per image");
+    return VFS_ERR_ARG;
+  }
+  if (count == 0 || n == 0) return VFS_OK;
+  if (!d_src || !d_dst) {
+    vfs::set_global_error("vfs_equalize_hist_u8_noalloc: null image pointer");
+    return VFS_ERR_ARG;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    (void)cudaGetLastError();
+    vfs::set_global_error("vfs_equalize_hist_u8_noalloc: no usable current device");
+    return VFS_ERR_CUDA;
+  }
+  unsigned char* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || !p) {
+        (void)cudaGetLastError();
+        vfs::set_global_error("vfs_equalize_hist_u8_noalloc: cudaGetSymbolAddress failed");
+        return VFS_ERR_CUDA;
+      }
+      g_noalloc_addr[dev] = p;
+    }
+    scratch = (unsigned char*)g_noalloc_addr[dev];
+  }
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  try {
+    for (int k = 0; k < count; k++) {
+      unsigned int* hist = (unsigned int*)(scratch + k * kSlotBytes);
+      uint8_t* lut = scratch + k * kSlotBytes + 256 * sizeof(unsigned int);
+      // launch_equalize_hist clears the histogram slot first (the array keeps the
+      // previous call's contents)
+      vfs::launch_equalize_hist(d_src + (size_t)k * n, d_dst + (size_t)k * n, n, hist, lut, st);
+    }
+  } catch (const vfs::CudaError&) {
+    (void)cudaGetLastError();
+    vfs::set_global_error("vfs_equalize_hist_u8_noalloc: launch failed");
+    return VFS_ERR_CUDA;
+  }
+  return VFS_OK;
+}
