@@ -115,6 +115,12 @@ int vfs_debug_get_buffer(vfs_stereo* s, const char* name, int comps, float* out)
 int vfs_set_solve_path(vfs_stereo* s, int path, int half_storage);
 int vfs_set_graph(vfs_stereo* s, int use_graph);
 
+/* Device memory a handle of this geometry allocates (solver state, plus the fused-path
+ * buffers when fused != 0), without allocating: for admission control.  0 for invalid
+ * geometry.  (No counterpart in the reference.) */
+size_t vfs_estimate_device_bytes(int width, int height, int nLevels, float fScale, int strideAlignment,
+                                 int fused);
+
 /* Batched solves: several handles (pairs, possibly of different sizes) solved together,
  * one launch per step and pyramid level for all of them, replayed as a CUDA graph.
  * Pairs of a batch need equal nWarpIters, nSolverIters and timestep_lambda.  The batch

@@ -75,6 +75,7 @@ SIGNATURES = {
     "vfs_batch_solve": [_vp, _i],
     "vfs_equalize_hist_u8": [_vp, _vp, _sz, _vp],
     "vfs_equalize_hist_u8_noalloc": [_vp, _vp, _sz, _i, _vp],
+    "vfs_estimate_device_bytes": [_i, _i, _i, _f, _i, _i],
     "vfs_launch_count": [],
     "vfs_profile_enable": [_vp, _i],
     "vfs_profile_reset": [_vp],
@@ -86,6 +87,7 @@ SIGNATURES = {
     "SolveStereo": [_vp, _vp, _vp, _vp, _i, _i, _f],
 }
 _RESTYPE = {
+    "vfs_estimate_device_bytes": ctypes.c_size_t,
     "vfs_launch_count": ctypes.c_longlong,
     "vfs_status_string": ctypes.c_char_p,
     "vfs_last_error": ctypes.c_char_p,

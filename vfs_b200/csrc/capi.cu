@@ -257,6 +257,10 @@ int vfs_set_graph(vfs_stereo* s, int use_graph) {
   return guarded(s, [&] { s->impl.engine.use_graph = use_graph != 0; });
 }
 
+size_t vfs_estimate_device_bytes(int width, int height, int nLevels, float fScale, int sa, int fused) {
+  return vfs::estimate_device_bytes(width, height, nLevels, fScale, sa, fused != 0);
+}
+
 int vfs_batch_create(vfs_batch** out) {
   if (!out) return VFS_ERR_ARG;
   *out = new (std::nothrow) vfs_batch();
@@ -308,6 +312,8 @@ int vfs_batch_clear(vfs_batch* b) {
     VFS_CUDA(cudaStreamSynchronize(b->stream));
     b->members.clear();
     b->engine.clear();
+    for (auto e : b->ready) cudaEventDestroy(e);
+    b->ready.clear();
   });
 }
 

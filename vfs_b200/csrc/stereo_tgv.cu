@@ -110,6 +110,40 @@ static int align_up(int n, int m) {
   return mod ? n + m - mod : n;
 }
 
+// pool: pyramid (5 planes/level: I0, I1, mask, tv x2); full-resolution planes:
+// 18 float, 10 float2, 1 float4, 2 float3, 1 four-plane staging; u8 and uchar3
+// image staging; 512 B alignment slack per buffer.
+static size_t pool_bytes_for(const std::vector<int>& pS, const std::vector<int>& pH, size_t full) {
+  size_t bytes = 0;
+  for (size_t l = 0; l < pS.size(); l++) bytes += (size_t)pS[l] * pH[l] * sizeof(float) * 5 + 4 * 512;
+  const size_t planes = 18 + 10 * 2 + 4 + 2 * 3 + 4;
+  return bytes + full * sizeof(float) * planes + full * (2 + 2 * 3) + 64 * 512;
+}
+
+// p, q two planes each (float: 8 + 16 bytes per pixel and plane), half v-bar pair, and
+// two edge-code bytes per pixel and level.
+static size_t fused_bytes_for(const std::vector<int>& pS, const std::vector<int>& pH, size_t full) {
+  size_t bytes = full * 2 * 8 + full * 2 * 16 + full * 4 * 2 + 8 * 512;
+  for (size_t l = 0; l < pS.size(); l++) bytes += 2 * ((size_t)pS[l] * pH[l] + 512);
+  return bytes;
+}
+
+size_t estimate_device_bytes(int width, int height, int nLevels, float fScale, int sa, bool fused) {
+  if (width <= 0 || height <= 0 || nLevels <= 0 || sa <= 0 || !(fScale > 0.0f)) return 0;
+  std::vector<int> pS, pH;
+  int nh = height, nw = width;
+  for (int l = 0; l < nLevels; l++) {
+    if (nw <= 0 || nh <= 0) return 0;
+    pS.push_back(align_up(nw, sa));
+    pH.push_back(nh);
+    nh = (int)((float)nh / fScale);
+    nw = (int)((float)nw / fScale);
+  }
+  size_t full = (size_t)pS[0] * pH[0];
+  if (full * 8 >= ((size_t)1 << 31)) return 0;  // initialize refuses this geometry
+  return pool_bytes_for(pS, pH, full) + (fused ? fused_bytes_for(pS, pH, full) : 0);
+}
+
 // stereotgv.cu:44-168
 void StereoTgvImpl::initialize(const SolverParams& p) {
   if (p.width <= 0 || p.height <= 0 || p.nLevels <= 0 || p.nWarpIters < 0 || p.nSolverIters < 0 ||
@@ -148,14 +182,7 @@ void StereoTgvImpl::initialize(const SolverParams& p) {
   if (full_ * 8 >= ((size_t)1 << 31))
     throw ArgError{"initialize: image too large (row pitch x height x 8 must stay below 2^31)"};
   size_t f = full_ * sizeof(float);
-  // pool: pyramid (5 planes/level: I0, I1, mask, tv x2); full-resolution planes:
-  // 18 float, 10 float2, 1 float4, 2 float3, 1 four-plane staging; u8 and uchar3
-  // image staging; 512 B alignment slack per buffer.
-  size_t bytes = 0;
-  for (int l = 0; l < p.nLevels; l++) bytes += (size_t)pS[l] * pH[l] * sizeof(float) * 5 + 4 * 512;
-  const size_t planes = 18 + 10 * 2 + 4 + 2 * 3 + 4;
-  bytes += f * planes + full_ * (2 + 2 * 3) + 64 * 512;
-  pool_bytes_ = bytes;
+  pool_bytes_ = pool_bytes_for(pS, pH, full_);
   cudaError_t e = cudaMalloc(&pool_, pool_bytes_);
   if (e != cudaSuccess) {
     pool_ = nullptr;
@@ -295,8 +322,7 @@ void StereoTgvImpl::solve(bool masked) {
 void StereoTgvImpl::ensureFused() {
   if (fpool_) return;
   size_t n = full_;
-  size_t bytes = n * 2 * 8 + n * 2 * 16 + n * 4 * 2 + 8 * 512;
-  for (int l = 0; l < levels(); l++) bytes += 2 * ((size_t)pS[l] * pH[l] + 512);
+  size_t bytes = fused_bytes_for(pS, pH, full_);
   cudaError_t e = cudaMalloc(&fpool_, bytes);
   if (e != cudaSuccess) {
     fpool_ = nullptr;

@@ -60,6 +60,10 @@ class FusedEngine {
   std::map<std::vector<uintptr_t>, Entry> cache_;
 };
 
+// Device bytes a pair of this geometry allocates: the solver pool, and with `fused`
+// also the fused-path buffers.  Matches StereoTgvImpl::initialize / ensureFused.
+size_t estimate_device_bytes(int width, int height, int nLevels, float fScale, int strideAlignment, bool fused);
+
 class StereoTgvImpl {
  public:
   StereoTgvImpl(int blockWidth, int blockHeight, int strideAlignment);
