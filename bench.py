@@ -45,6 +45,9 @@ def parse():
     ap.add_argument("--storage", default="fp16", choices=["fp16", "fp32"], help="fused path: p, q, v-bar storage")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in comparison run")
     ap.add_argument("--seed", type=int, default=20260)
+    ap.add_argument("--mode", default="frames", choices=["frames", "mixed", "serving"],
+                    help="frames: 848x800 batch (headline); mixed: 8x848x800 + 4x640x480 + 4x424x400 in one "
+                         "batch; serving: 6 camera streams with Poisson arrivals")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -57,7 +60,8 @@ def dist_env():
 
 
 def pair_cache(w, h, seed):
-    """Synthetic pair, cached under /tmp so repeated runs on one machine skip rendering."""
+    """Synthetic pair (rendered on the GPU when there is one), cached under /tmp so repeated
+    runs on one machine skip rendering."""
     from vfs_b200 import synth
     path = f"/tmp/vfs_b200_pair_{w}x{h}_{seed}.npz"
     if os.path.exists(path):
@@ -66,7 +70,12 @@ def pair_cache(w, h, seed):
             return dict(i0=d["i0"], i1=d["i1"], mask=d["mask"], tv=d["tv"], cv=d["cv"])
         except Exception:
             pass
-    p = synth.make_pair(w, h, seed)
+    try:
+        import torch
+        gpu = torch.cuda.is_available()
+    except Exception:
+        gpu = False
+    p = synth.make_pair_gpu(w, h, seed) if gpu else synth.make_pair(w, h, seed)
     d = dict(i0=p.i0, i1=p.i1, mask=p.mask, tv=p.tv, cv=p.cv)
     try:
         np.savez(path, **d)
@@ -447,11 +456,147 @@ def run_ours(args, rank, world, local):
     return result
 
 
+def run_mixed(args):
+    """Uneven batch: 8 x 848x800 + 4 x 640x480 + 4 x 424x400 pairs in one batched fused solve
+    (float storage), checked per pair against the drop-in path."""
+    import torch
+    from vfs_b200 import synth
+    from vfs_b200.build import build
+    from vfs_b200.stereotgv import StereoBatch, StereoTgv
+    build()
+    dev = torch.device("cuda", 0)
+    sizes = [(848, 800)] * 8 + [(640, 480)] * 4 + [(424, 400)] * 4
+    sp = synth.SOLVER_PARAMS
+    stream = torch.cuda.Stream(device=dev)
+    pairs, solvers = [], []
+    batch = StereoBatch(half_storage=False, stream=stream)
+    for k, (w, h) in enumerate(sizes):
+        p = pair_cache(w, h, args.seed + 100 + k)
+        s = StereoTgv()
+        s.set_solve_path(True, False)
+        s.limitRange = synth.LIMIT_RANGE
+        s.initialize(w, h, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"],
+                     sp["lambda_"], synth.n_levels_for(w), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+        s.copyMaskToDevice(p["mask"])
+        s.loadVectorFields(p["tv"], p["cv"])
+        s.set_stream(stream)
+        batch.add(s)
+        pairs.append(p)
+        solvers.append(s)
+    d_imgs = [(torch.from_numpy(p["i0"]).to(dev), torch.from_numpy(p["i1"]).to(dev)) for p in pairs]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def step():
+        for s, (a, b) in zip(solvers, d_imgs):
+            s.copy_images_from_device(a, b)
+        batch.solve(True)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    # parity per size class: one more frame, against the drop-in path on a fresh handle pair
+    worst = 0.0
+    for k in (0, 8, 12):
+        w, h = sizes[k]
+        ref = StereoTgv()
+        ref.limitRange = synth.LIMIT_RANGE
+        ref.initialize(w, h, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"],
+                       sp["lambda_"], synth.n_levels_for(w), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+        ref.copyMaskToDevice(pairs[k]["mask"])
+        ref.loadVectorFields(pairs[k]["tv"], pairs[k]["cv"])
+        mine = StereoTgv()
+        mine.set_solve_path(True, False)
+        mine.limitRange = synth.LIMIT_RANGE
+        mine.initialize(w, h, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"],
+                        sp["lambda_"], synth.n_levels_for(w), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+        mine.copyMaskToDevice(pairs[k]["mask"])
+        mine.loadVectorFields(pairs[k]["tv"], pairs[k]["cv"])
+        ref.copyImagesToDevice(pairs[k]["i0"], pairs[k]["i1"])
+        ref.solveStereoForwardMasked()
+        # the batch member has solved warmup + steps frames; solve a fresh fused handle once
+        mine.copyImagesToDevice(pairs[k]["i0"], pairs[k]["i1"])
+        mine.solveStereoForwardMasked()
+        worst = max(worst, float(np.abs(ref.copy1DDisparityToHost() - mine.copy1DDisparityToHost()).max()))
+    per_step = float(np.mean(ms))
+    print(json.dumps({
+        "metric": "mixed-size stereo frames/s (one batched fused solve per step)", "value": 16000.0 / per_step,
+        "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "8x848x800 + 4x640x480 + 4x424x400 pairs, masked solve, 3 warps x 50 iterations",
+                   "storage": "fp32", "l2": "flushed (256 MiB write) before every step"},
+        "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+        "max_abs_vs_plain_px": worst,
+    }), flush=True)
+
+
+def run_serving(args):
+    """6 camera streams (4 x 848x800, 2 x 424x400), 120 frames each along smooth random
+    trajectories, Poisson arrivals totalling 180 requests/s, served by the continuous-batching
+    server (fused, FP16 storage) and by the drop-in path one request at a time."""
+    import torch
+    from vfs_b200 import synth
+    from vfs_b200.build import build
+    from vfs_b200.serving import StereoServer, poisson_schedule, replay
+    build()
+    n_frames = max(8, min(120, args.steps * 12))
+    cams = [(0, 848, 800), (1, 848, 800), (2, 848, 800), (3, 848, 800), (4, 424, 400), (5, 424, 400)]
+    data = {}
+    for sid, w, h in cams:
+        fields, frames = synth.make_sequence_gpu(w, h, args.seed + 7 * sid, n_frames)
+        data[sid] = (w, h, fields, frames)
+    rates = {sid: 30.0 for sid, _, _ in cams}
+    sched = poisson_schedule(rates, {sid: n_frames for sid, _, _ in cams}, seed=args.seed)
+    sp = synth.SOLVER_PARAMS
+    params = dict(sp, limitRange=synth.LIMIT_RANGE)
+    out = {}
+    for label, kw in (("fused_fp16_batched", dict(path="fused", half_storage=True, max_batch=8, lanes=2)),
+                      ("plain_fp32_one_at_a_time", dict(path="plain"))):
+        srv = StereoServer(reserve_bytes=1 << 30, **kw)
+        for sid, (w, h, fields, frames) in data.items():
+            srv.open_stream(sid, w, h, fields["mask"], fields["tv"], fields["cv"], synth.n_levels_for(w), params)
+        # warm the server (graphs off, kernels loaded, tuning done) with one frame per stream
+        for sid, (w, h, fields, frames) in data.items():
+            srv.submit(sid, *frames[0])
+        srv.run_until_idle()
+        srv.done.clear()
+        t_start = time.perf_counter()
+        replay(srv, sched, {sid: d[3] for sid, d in data.items()}, realtime=True)
+        st = srv.stats(since=t_start)
+        st["arrival_rate_per_s"] = 180.0
+        out[label] = st
+        del srv
+        torch.cuda.synchronize()
+    line = {"metric": "serving: 6 camera streams, 180 requests/s Poisson, p50/p99 latency and frames/s",
+            "value": out["fused_fp16_batched"].get("frames_per_s"), "unit": "frames/s", "n_gpus": 1,
+            "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "4 x 848x800 + 2 x 424x400 streams, %d frames each, 30 req/s each" % n_frames},
+            "serving": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.mode == "mixed":
+        if rank == 0:
+            run_mixed(args)
+        return
+    if args.mode == "serving":
+        if rank == 0:
+            run_serving(args)
         return
     run_ours(args, rank, world, local)
 

@@ -138,6 +138,11 @@ int vfs_batch_size(const vfs_batch* b);
 int vfs_batch_set_storage(vfs_batch* b, int half_storage);
 int vfs_batch_set_graph(vfs_batch* b, int use_graph);
 int vfs_batch_solve(vfs_batch* b, int masked);
+/* The fused path picks the tile height of its iteration kernel per pyramid level by timing
+ * the variants on the first solve of each batch composition (on by default); the timing
+ * launches do not change results.  Off: the default 31 x 8 tiles everywhere. */
+int vfs_batch_set_autotune(vfs_batch* b, int on);
+int vfs_set_autotune(vfs_stereo* s, int on);
 
 /* Histogram equalisation of n 8-bit pixels in device memory (d_dst may equal d_src), as
  * cv::equalizeHist, which the reference's SolveStereo applies to both images on the host

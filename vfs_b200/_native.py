@@ -73,6 +73,8 @@ SIGNATURES = {
     "vfs_batch_set_storage": [_vp, _i],
     "vfs_batch_set_graph": [_vp, _i],
     "vfs_batch_solve": [_vp, _i],
+    "vfs_batch_set_autotune": [_vp, _i],
+    "vfs_set_autotune": [_vp, _i],
     "vfs_equalize_hist_u8": [_vp, _vp, _sz, _vp],
     "vfs_equalize_hist_u8_noalloc": [_vp, _vp, _sz, _i, _vp],
     "vfs_estimate_device_bytes": [_i, _i, _i, _f, _i, _i],

@@ -4,6 +4,7 @@
 // pair.  Pairs may differ in size and pyramid depth; a pair joins the schedule at
 // its own coarsest level.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -22,15 +23,19 @@ void set_tiles(ArgsT& A, int k, int w, int h) {
   A.ntiles += tiles_of(w, h);
 }
 
-void set_iter_tiles(IterArgs& A, int k, int w, int h) {
+void set_iter_tiles(IterArgs& A, int k, int w, int h, int rows) {
   A.pr[k].tiles_x = iter_tiles_x_of(w);
   A.pr[k].tile0 = A.ntiles;
-  A.ntiles += iter_tiles_of(w, h);
+  A.ntiles += iter_tiles_of(w, h, rows);
 }
 
 }  // namespace
 
-void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st) {
+// level_variant[l]: tile variant of the iteration kernel at level l; -1 = time the
+// variants on this level's data before its first iteration (only when can_tune) and
+// store the fastest there.
+void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st,
+                        std::vector<int>& level_variant, bool can_tune) {
   const int n = (int)pairs.size();
   if (n == 0) return;
   if (n > kMaxPairs) throw ArgError{"batch larger than " + std::to_string(kMaxPairs) + " pairs"};
@@ -154,18 +159,12 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         launch_derivatives_batched(Dv, st);
       }
       prof->profEnd();
-      float tau = 1.0f;
-      float sigma = 1.0f / tau;
-      prof->profBeginPx(kProfFused, px_level, P0.nSolverIters);
-      for (int iter = 0; iter < P0.nSolverIters; iter++) {
-        float mu;
-        if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P0.timestep_lambda);
-        else mu = 1;
+      auto iter_args = [&](int variant, float sigma_, float tau_, float mu_, int write_tp) {
         IterArgs A{};
-        A.sigma = sigma;
-        A.tau = tau;
-        A.mu = mu;
-        A.write_tp = iter == P0.nSolverIters - 1;
+        A.sigma = sigma_;
+        A.tau = tau_;
+        A.mu = mu_;
+        A.write_tp = write_tp;
         for (int k = 0; k < na; k++) {
           StereoTgvImpl* s = act[k];
           IterPair& d = A.pr[k];
@@ -191,12 +190,56 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
           d.alpha1 = s->P.alpha1;
           d.lambda = s->P.lambda;
           // updateDualVariables.cu:174-176, 217: uniform per launch, evaluated here in float
-          A.sp[k] = s->P.alpha1 * sigma / 3.0f;
-          A.sq[k] = s->P.alpha0 * sigma / 2.0f;
-          set_iter_tiles(A, k, d.w, d.h);
+          A.sp[k] = s->P.alpha1 * sigma_ / 3.0f;
+          A.sq[k] = s->P.alpha0 * sigma_ / 2.0f;
+          set_iter_tiles(A, k, d.w, d.h, kIterVariantRows[variant]);
         }
         A.npairs = na;
-        launch_fused_iteration(A, masked, half, st, iter & 1);
+        return A;
+      };
+      if (level_variant[level] < 0) {
+        if (can_tune && warpIter == 0 && P0.nSolverIters > 0) {
+          // Time every tile variant on this level's data.  These launches read the same
+          // inputs as the first iteration below and write only what it overwrites (the
+          // other p / q plane, us, u_s, v_s at in-mask pixels; T p is left alone), so they
+          // do not change any result.
+          float best = 1e30f;
+          int best_v = kIterDefaultVariant;
+          float mu0 = 1.0f / std::sqrt(1 + 0.7f * 1.0f * P0.timestep_lambda);
+          cudaEvent_t e0, e1;
+          VFS_CUDA(cudaEventCreate(&e0));
+          VFS_CUDA(cudaEventCreate(&e1));
+          for (int v = 0; v < kIterVariants; v++) {
+            IterArgs T = iter_args(v, 1.0f, 1.0f, mu0, 0);
+            launch_fused_iteration(T, masked, half, st, 0, v);  // warm the caches / the instruction path
+            VFS_CUDA(cudaEventRecord(e0, st));
+            for (int r = 0; r < 3; r++) launch_fused_iteration(T, masked, half, st, 0, v);
+            VFS_CUDA(cudaEventRecord(e1, st));
+            VFS_CUDA(cudaEventSynchronize(e1));
+            float ms = 0;
+            VFS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (ms < best) {
+              best = ms;
+              best_v = v;
+            }
+          }
+          cudaEventDestroy(e0);
+          cudaEventDestroy(e1);
+          level_variant[level] = best_v;
+        } else if (!can_tune) {
+          level_variant[level] = kIterDefaultVariant;
+        }
+      }
+      const int variant = level_variant[level] < 0 ? kIterDefaultVariant : level_variant[level];
+      float tau = 1.0f;
+      float sigma = 1.0f / tau;
+      prof->profBeginPx(kProfFused, px_level, P0.nSolverIters);
+      for (int iter = 0; iter < P0.nSolverIters; iter++) {
+        float mu;
+        if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P0.timestep_lambda);
+        else mu = 1;
+        IterArgs A = iter_args(variant, sigma, tau, mu, iter == P0.nSolverIters - 1);
+        launch_fused_iteration(A, masked, half, st, iter & 1, variant);
         for (auto* s : act) {
           std::swap(s->d_u, s->d_us);
           std::swap(s->d_u_, s->d_u_s);
@@ -313,12 +356,36 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
 void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st) {
   if (pairs.empty()) return;
   prepare(pairs, masked);
+  // tile variants per level for this batch composition (tuned on its first solve)
+  // key: form, storage and the multiset of pair geometries (order does not change the work)
+  std::vector<std::array<int, 3>> geo;
+  int maxL = 0;
+  for (auto* s : pairs) {
+    geo.push_back({s->width, s->height, s->levels()});
+    maxL = std::max(maxL, s->levels());
+  }
+  std::sort(geo.begin(), geo.end());
+  std::vector<int> comp{(int)masked, (int)half};
+  for (auto& g : geo) comp.insert(comp.end(), g.begin(), g.end());
+  auto tit = tuned_.find(comp);
+  if (tit == tuned_.end()) {
+    std::vector<int> lv(maxL, autotune ? -1 : kIterDefaultVariant);
+    if (autotune) {
+      // first solve of this composition: run it directly and tune while it runs
+      fused_solve_direct(pairs, masked, half, st, lv, true);
+      tuned_[comp] = lv;
+      return;
+    }
+    tit = tuned_.emplace(comp, lv).first;
+  }
+  std::vector<int> variants = tit->second;
   if (!use_graph) {
-    fused_solve_direct(pairs, masked, half, st);
+    fused_solve_direct(pairs, masked, half, st, variants, false);
     return;
   }
   StereoTgvImpl* prof = pairs[0];
   std::vector<uintptr_t> key{(uintptr_t)masked, (uintptr_t)half, (uintptr_t)prof->profiling};
+  for (int v : variants) key.push_back((uintptr_t)v);
   std::vector<PairPtrs> before;
   for (auto* s : pairs) {
     PairPtrs p = get_ptrs(s);
@@ -340,7 +407,7 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     cudaGraph_t g = nullptr;
     VFS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
     try {
-      fused_solve_direct(pairs, masked, half, st);
+      fused_solve_direct(pairs, masked, half, st, variants, false);
     } catch (...) {
       prof->capture_events = nullptr;
       cudaGraph_t junk = nullptr;

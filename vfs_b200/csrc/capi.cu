@@ -327,6 +327,14 @@ int vfs_batch_set_graph(vfs_batch* b, int use_graph) {
   return guarded(b, [&] { b->engine.use_graph = use_graph != 0; });
 }
 
+int vfs_batch_set_autotune(vfs_batch* b, int on) {
+  return guarded(b, [&] { b->engine.autotune = on != 0; });
+}
+
+int vfs_set_autotune(vfs_stereo* s, int on) {
+  return guarded(s, [&] { s->impl.engine.autotune = on != 0; });
+}
+
 int vfs_batch_solve(vfs_batch* b, int masked) {
   return guarded(b, [&] {
     if (b->members.empty()) throw vfs::ArgError{"batch solve: empty batch"};

@@ -79,8 +79,10 @@ struct IterArgs {
   int write_tp;
   IterPair pr[kMaxPairs];
 };
-// parity selects which half of the p / q ping-pong buffers is read (the other is written)
-void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity);
+// parity selects which half of the p / q ping-pong buffers is read (the other is written);
+// variant selects the tile height (kIterVariantRows[variant] rows of 31 pixels).
+void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
+                            int variant);
 
 // ---- per-warp prologue: zero p, q, v-bar; resample tv at x + warpUV; warp I1 ----
 struct WarpStartPair {
@@ -183,15 +185,14 @@ void launch_edge_codes(const float* mask, uint8_t* code, int w, int h, int s, cu
 inline int tiles_x_of(int w) { return (w + kFTW - 1) / kFTW; }
 inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFTH); }
 // the iteration kernel's tiles: 31 x kIterTH pixels (a 32 x (kIterTH + 1) block with halo)
-#ifndef VFS_ITER_TH
-#define VFS_ITER_TH 8
-#endif
-#ifndef VFS_ITER_MINB
-#define VFS_ITER_MINB 7
-#endif
-constexpr int kIterTH = VFS_ITER_TH;
-constexpr int kIterMinBlocks = VFS_ITER_MINB;  // __launch_bounds__ minimum resident blocks per SM
+// Tile-height variants of the iteration kernel (chosen per level by the autotuner in
+// FusedEngine): rows per tile and the minimum resident blocks per SM its launch bounds
+// ask for (which caps registers at 32 or 40 per thread).
+constexpr int kIterVariants = 3;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3};
+constexpr int kIterDefaultVariant = 1;
 inline int iter_tiles_x_of(int w) { return (w + 30) / 31; }
-inline int iter_tiles_of(int w, int h) { return iter_tiles_x_of(w) * ((h + kIterTH - 1) / kIterTH); }
+inline int iter_tiles_of(int w, int h, int rows) { return iter_tiles_x_of(w) * ((h + rows - 1) / rows); }
 
 }  // namespace vfs

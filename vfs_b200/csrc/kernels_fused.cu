@@ -83,9 +83,8 @@ struct FusedIter {
 // evaluates the dual update at its region pixel; after a barrier the tile threads
 // finish the threshold and primal steps with the west / north values from shared
 // memory.
-template <bool MASKED, class ST, int TH>
-__global__ void __launch_bounds__(32 * (TH + 1), kIterMinBlocks) k_fused_iter(const __grid_constant__ IterArgs A,
-                                                                              int parity) {
+template <bool MASKED, class ST, int TH, int MINB>
+__global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid_constant__ IterArgs A, int parity) {
   typedef FusedIter<MASKED, ST> F;
   typedef typename F::T2 T2;
   typedef typename F::T4 T4;
@@ -187,16 +186,26 @@ __global__ void __launch_bounds__(32 * (TH + 1), kIterMinBlocks) k_fused_iter(co
   S::st2((T2*)P.v_s, pos, vs);
 }
 
-void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity) {
-  constexpr int TH = kIterTH;
+template <int TH, int MINB>
+static void launch_iter_th(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity) {
   dim3 blk(32, TH + 1);
-  if (A.ntiles <= 0) return;
   if (masked) {
-    if (half_storage) k_fused_iter<true, __half, TH><<<A.ntiles, blk, 0, st>>>(A, parity);
-    else k_fused_iter<true, float, TH><<<A.ntiles, blk, 0, st>>>(A, parity);
+    if (half_storage) k_fused_iter<true, __half, TH, MINB><<<A.ntiles, blk, 0, st>>>(A, parity);
+    else k_fused_iter<true, float, TH, MINB><<<A.ntiles, blk, 0, st>>>(A, parity);
   } else {
-    if (half_storage) k_fused_iter<false, __half, TH><<<A.ntiles, blk, 0, st>>>(A, parity);
-    else k_fused_iter<false, float, TH><<<A.ntiles, blk, 0, st>>>(A, parity);
+    if (half_storage) k_fused_iter<false, __half, TH, MINB><<<A.ntiles, blk, 0, st>>>(A, parity);
+    else k_fused_iter<false, float, TH, MINB><<<A.ntiles, blk, 0, st>>>(A, parity);
+  }
+}
+
+void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
+                            int variant) {
+  if (A.ntiles <= 0) return;
+  static_assert(kIterVariantRows[0] == 4 && kIterVariantRows[1] == 8 && kIterVariantRows[2] == 16, "variants");
+  switch (variant) {
+    case 0: launch_iter_th<4, kIterVariantMinBlocks[0]>(A, masked, half_storage, st, parity); break;
+    case 2: launch_iter_th<16, kIterVariantMinBlocks[2]>(A, masked, half_storage, st, parity); break;
+    default: launch_iter_th<8, kIterVariantMinBlocks[1]>(A, masked, half_storage, st, parity); break;
   }
   VFS_LAUNCH_CHECK();
 }

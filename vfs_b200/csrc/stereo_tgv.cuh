@@ -43,6 +43,9 @@ struct PairPtrs {
 class FusedEngine {
  public:
   bool use_graph = true;
+  bool autotune = true;  // pick the iteration kernel's tile variant per level on first use
+  // tuned tile variant per level, keyed by batch composition (form, storage, sizes)
+  const std::map<std::vector<int>, std::vector<int>>& tuned() const { return tuned_; }
   ~FusedEngine();
   void clear();
   void solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st);
@@ -58,6 +61,7 @@ class FusedEngine {
     std::vector<cudaEvent_t> events;
   };
   std::map<std::vector<uintptr_t>, Entry> cache_;
+  std::map<std::vector<int>, std::vector<int>> tuned_;
 };
 
 // Device bytes a pair of this geometry allocates: the solver pool, and with `fused`

@@ -1,0 +1,66 @@
+"""A small, self-contained solve for profilers: one batched fused solve of `--batch` seeded
+848x800 pairs (no CUDA graph, so every kernel is an ordinary launch).
+
+    python -m vfs_b200.profile_case --batch 4 --half 1 [--frames 1] [--path fused|plain]
+
+Launch order per frame: pyramid, then per level (coarse to fine) the level kernels and
+per warp the prologue, the 50 fused iterations and the epilogue, so the first fused
+iteration at full resolution comes after 4 x 150 = 600 fused launches.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+
+import numpy as np
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--batch", type=int, default=4)
+    ap.add_argument("--half", type=int, default=1)
+    ap.add_argument("--frames", type=int, default=1)
+    ap.add_argument("--path", default="fused", choices=["fused", "plain"])
+    ap.add_argument("--width", type=int, default=848)
+    ap.add_argument("--height", type=int, default=800)
+    a = ap.parse_args()
+    from . import synth
+    from .stereotgv import StereoBatch, StereoTgv
+    w, h = a.width, a.height
+    cache = f"/tmp/vfs_b200_pair_{w}x{h}_7.npz"
+    if os.path.exists(cache):
+        d = dict(np.load(cache))
+    else:
+        p = synth.make_pair(w, h, 7)
+        d = dict(i0=p.i0, i1=p.i1, mask=p.mask, tv=p.tv, cv=p.cv)
+        np.savez(cache, **d)
+    sp = synth.SOLVER_PARAMS
+    fused = a.path == "fused"
+    batch = StereoBatch(half_storage=bool(a.half)) if fused else None
+    if batch is not None:
+        batch.set_graph(False)
+    solvers = []
+    for _ in range(a.batch if fused else 1):
+        s = StereoTgv()
+        s.set_solve_path(fused, bool(a.half) and fused)
+        s.limitRange = synth.LIMIT_RANGE
+        s.initialize(w, h, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"],
+                     sp["lambda_"], synth.n_levels_for(w), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+        s.copyMaskToDevice(d["mask"])
+        s.loadVectorFields(d["tv"], d["cv"])
+        if batch is not None:
+            batch.add(s)
+        solvers.append(s)
+    for _ in range(a.frames):
+        for s in solvers:
+            s.copyImagesToDevice(d["i0"], d["i1"])
+        if batch is not None:
+            batch.solve(True)
+        else:
+            solvers[0].solveStereoForwardMasked()
+    u = solvers[0].copy1DDisparityToHost()
+    print("done", float(u[h // 2, w // 2]))
+
+
+if __name__ == "__main__":
+    main()

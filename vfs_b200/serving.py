@@ -80,11 +80,15 @@ DEFAULT_PARAMS = dict(beta=10.0, gamma=0.8, alpha0=17.0, alpha1=1.2, timestep_la
 
 class StereoServer:
     def __init__(self, device: int = 0, max_batch: int = 8, lanes: int = 2, half_storage: bool = True,
-                 reserve_bytes: int = 1 << 30, use_graph: bool = False):
+                 reserve_bytes: int = 1 << 30, use_graph: bool = False, path: str = "fused"):
+        """path="plain" serves one request at a time with the drop-in path (the baseline)."""
         import torch
         self.torch = torch
         self.device = torch.device("cuda", device)
         torch.cuda.set_device(self.device)
+        self.path = path
+        if path == "plain":
+            max_batch, half_storage = 1, False
         self.max_batch = max_batch
         self.half = half_storage
         self.reserve = reserve_bytes
@@ -94,6 +98,7 @@ class StereoServer:
         for _ in range(lanes):
             b = StereoBatch(half_storage=half_storage)
             b.set_graph(use_graph)
+            b.set_autotune(False)  # compositions change every launch: no per-composition timing passes
             st = torch.cuda.Stream(device=self.device)
             b.set_stream(st)
             self.lanes.append(_Lane(stream=st, batch=b))
@@ -110,12 +115,13 @@ class StereoServer:
         if stream_id in self.cameras:
             raise ValueError(f"stream {stream_id} already open")
         p = dict(DEFAULT_PARAMS, **(params or {}))
-        need = self.footprint(width, height, n_levels, p["fScale"])
+        need = int(lib().vfs_estimate_device_bytes(width, height, n_levels, p["fScale"], 32,
+                                                   0 if self.path == "plain" else 1))
         free, _ = self.torch.cuda.mem_get_info(self.device)
         if need == 0 or need + self.reserve > free:
             raise AdmissionError(f"stream {stream_id}: needs {need} bytes + reserve {self.reserve}, free {free}")
         s = StereoTgv()
-        s.set_solve_path(True, self.half)
+        s.set_solve_path(self.path != "plain", self.half)
         s.limitRange = p["limitRange"]
         s.initialize(width, height, p["beta"], p["gamma"], p["alpha0"], p["alpha1"], p["timestep_lambda"],
                      p["lambda_"], n_levels, p["fScale"], p["nWarpIters"], p["nSolverIters"])
@@ -188,9 +194,13 @@ class StereoServer:
                 a = torch.from_numpy(np.ascontiguousarray(r.i0)).pin_memory().to(self.device, non_blocking=True)
                 b = torch.from_numpy(np.ascontiguousarray(r.i1)).pin_memory().to(self.device, non_blocking=True)
                 cam.solver.copy_images_from_device(a, b)
-                lane.batch.add(cam.solver)
+                if self.path != "plain":
+                    lane.batch.add(cam.solver)
                 r.t_launch = now
-            lane.batch.solve(True)
+            if self.path == "plain":
+                self.cameras[picked[0].stream_id].solver.solveStereoForwardMasked()
+            else:
+                lane.batch.solve(True)
             for r in picked:
                 cam = self.cameras[r.stream_id]
                 out = torch.empty((cam.height, cam.width), dtype=torch.float32, device=self.device)

@@ -83,6 +83,9 @@ class StereoTgv:
     def set_graph(self, on: bool) -> None:
         check(self._h, self._L.vfs_set_graph(self._h, int(on)))
 
+    def set_autotune(self, on: bool) -> None:
+        check(self._h, self._L.vfs_set_autotune(self._h, int(on)))
+
     # ---- reference methods -------------------------------------------------
     def initialize(self, width, height, beta, gamma, alpha0, alpha1, timestep_lambda, lambda_,
                    nLevels, fScale, nWarpIters, nSolverIters) -> int:
@@ -254,6 +257,9 @@ class StereoBatch:
 
     def set_graph(self, on: bool) -> None:
         check_batch(self._h, self._L.vfs_batch_set_graph(self._h, int(on)))
+
+    def set_autotune(self, on: bool) -> None:
+        check_batch(self._h, self._L.vfs_batch_set_autotune(self._h, int(on)))
 
     def add(self, solver: "StereoTgv") -> None:
         check_batch(self._h, self._L.vfs_batch_add(self._h, solver.handle))

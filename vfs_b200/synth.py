@@ -202,3 +202,141 @@ def make_sequence(width: int, height: int, seed: int, n_frames: int, max_step_m:
             R = R @ rotation_matrix(rng.normal(size=3), np.deg2rad(rng.uniform(0.0, max_step_deg)))
 
     return fields, frames()
+
+
+# ---- the same renderer on the GPU (torch), for long frame sequences ---------------------
+# Same scene, noise and camera model as `render`; transcendental functions come from torch,
+# so pixels can differ from the numpy renderer by one grey level.  Used for the serving
+# workload (hundreds of frames), not for test fixtures.
+def _hash3_t(ix, iy, iz, seed):
+    import torch
+    m = 0xFFFFFFFF
+    h = (ix * 0x9E3779B1) ^ (iy * 0x85EBCA77) ^ (iz * 0xC2B2AE3D) ^ (seed * 0x27D4EB2F + 0x165667B1)
+    h = h & m
+    h = h ^ (h >> 15)
+    h = (h * 0x2C1B3C6D) & m
+    h = h ^ (h >> 12)
+    h = (h * 0x297A2D39) & m
+    h = h ^ (h >> 15)
+    return h.to(torch.float64) / 4294967296.0
+
+
+def _value_noise3_t(P, freq, seed):
+    import torch
+    X = P * freq
+    i = torch.floor(X)
+    f = X - i
+    f = f * f * (3 - 2 * f)
+    i = i.to(torch.int64)
+    out = torch.zeros(P.shape[:-1], dtype=torch.float64, device=P.device)
+    for dx in (0, 1):
+        wx = f[..., 0] if dx else 1 - f[..., 0]
+        for dy in (0, 1):
+            wy = f[..., 1] if dy else 1 - f[..., 1]
+            for dz in (0, 1):
+                wz = f[..., 2] if dz else 1 - f[..., 2]
+                out = out + wx * wy * wz * _hash3_t(i[..., 0] + dx, i[..., 1] + dy, i[..., 2] + dz, seed)
+    return out
+
+
+def render_t(scene: Scene, rays_cam, R_wc, C, gen, noise_sigma=2.0 / 255.0):
+    """GPU render: rays_cam = unit rays of the camera (H x W x 3 torch float64 on the device)."""
+    import torch
+    dev = rays_cam.device
+    R = torch.as_tensor(np.asarray(R_wc, np.float64), device=dev)
+    Ct = torch.as_tensor(np.asarray(C, np.float64), device=dev)
+    d = rays_cam @ R.T
+    t = torch.full(d.shape[:-1], float("inf"), dtype=torch.float64, device=dev)
+    for n, c in scene.planes:
+        nt = torch.as_tensor(n, device=dev)
+        den = d @ nt
+        num = c - float(Ct @ nt)
+        tt = torch.where(den > 1e-6, num / den, torch.full_like(den, float("inf")))
+        tt = torch.where(tt > 0.3, tt, torch.full_like(tt, float("inf")))
+        t = torch.minimum(t, tt)
+    for cen, r in scene.spheres:
+        oc = Ct - torch.as_tensor(cen, device=dev)
+        b = d @ oc
+        disc = b * b - (float(oc @ oc) - r * r)
+        sq = torch.sqrt(torch.clamp(disc, min=0))
+        tt = torch.where(disc > 0, -b - sq, torch.full_like(b, float("inf")))
+        tt = torch.where(tt > 0.3, tt, torch.full_like(tt, float("inf")))
+        t = torch.minimum(t, tt)
+    b = d @ Ct
+    disc = b * b - (float(Ct @ Ct) - scene.bg_radius ** 2)
+    tb = -b + torch.sqrt(torch.clamp(disc, min=0))
+    t = torch.clamp(torch.minimum(t, tb), 0.5, scene.bg_radius)
+    P = Ct + d * t[..., None]
+    v = torch.zeros_like(t)
+    amp, tot = 1.0, 0.0
+    for k in range(5):
+        v = v + amp * _value_noise3_t(P, 3.0 * 2 ** k, scene.seed * 7 + k)
+        tot += amp
+        amp *= 0.5
+    val = 0.12 + 0.76 * (v / tot)
+    for lo, hi, off in scene.boxes:
+        lo_t = torch.as_tensor(lo, device=dev)
+        hi_t = torch.as_tensor(hi, device=dev)
+        inside = torch.all((P >= lo_t) & (P <= hi_t), dim=-1)
+        val = val + off * inside.to(torch.float64)
+    val = torch.clamp(val, 0.0, 1.0)
+    noise = torch.randn(t.shape, generator=gen, dtype=torch.float64, device=dev) * noise_sigma
+    img = torch.clamp(torch.round((val + noise) * 255.0), 0, 255).to(torch.uint8)
+    return img
+
+
+def make_sequence_gpu(width: int, height: int, seed: int, n_frames: int, device="cuda", max_step_m: float = 0.05,
+                      max_step_deg: float = 3.0, baseline: float = 0.064, max_rot_deg: float = 2.0,
+                      fov_deg: float = 163.0):
+    """Like make_sequence, rendered on the GPU: returns (fields dict, list of (i0, i1) uint8 numpy)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    scene = Scene.random(rng, seed)
+    cam = EquidistantCamera(width, height)
+    R01 = rotation_matrix(rng.normal(size=3), np.deg2rad(rng.uniform(0.0, max_rot_deg)))
+    b = np.array([baseline, 0.0, 0.0])
+    fields = dict(mask=fisheye_mask(cam, fov_deg), tv=translation_field(cam, b), cv=calibration_field(cam, cam, R01))
+    v, u = np.mgrid[0:height, 0:width].astype(np.float64)
+    rays = torch.as_tensor(cam.unproject(u, v), device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    R = np.eye(3)
+    C = np.zeros(3)
+    vel = rng.normal(size=3)
+    vel *= max_step_m * 0.7 / np.linalg.norm(vel)
+    frames = []
+    for _ in range(n_frames):
+        i0 = render_t(scene, rays, R, C, gen).cpu().numpy()
+        i1 = render_t(scene, rays, R @ R01, C + R @ b, gen).cpu().numpy()
+        frames.append((i0, i1))
+        vel = vel + rng.normal(size=3) * max_step_m * 0.2
+        nv = np.linalg.norm(vel)
+        if nv > max_step_m:
+            vel *= max_step_m / nv
+        Cn = C + vel
+        if np.linalg.norm(Cn) < 1.0:
+            C = Cn
+        else:
+            vel = -vel
+        R = R @ rotation_matrix(rng.normal(size=3), np.deg2rad(rng.uniform(0.0, max_step_deg)))
+    return fields, frames
+
+
+def make_pair_gpu(width: int, height: int, seed: int, device="cuda", baseline: float = 0.064,
+                  max_rot_deg: float = 2.0, fov_deg: float = 163.0) -> StereoPair:
+    """make_pair's scene, rotation and fields, with the two images rendered on the GPU."""
+    import torch
+    rng = np.random.default_rng(seed)
+    scene = Scene.random(rng, seed)
+    cam = EquidistantCamera(width, height)
+    axis = rng.normal(size=3)
+    R01 = rotation_matrix(axis, np.deg2rad(rng.uniform(0.0, max_rot_deg)))
+    b = np.array([baseline, 0.0, 0.0])
+    v, u = np.mgrid[0:height, 0:width].astype(np.float64)
+    rays = torch.as_tensor(cam.unproject(u, v), device=device)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    i0 = render_t(scene, rays, np.eye(3), np.zeros(3), gen).cpu().numpy()
+    i1 = render_t(scene, rays, R01, b, gen).cpu().numpy()
+    return StereoPair(i0=i0, i1=i1, mask=fisheye_mask(cam, fov_deg), tv=translation_field(cam, b),
+                      cv=calibration_field(cam, cam, R01), depth=None, seed=seed)
