@@ -405,6 +405,7 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     prof->profReset();
     prof->capture_events = &e.events;
     cudaGraph_t g = nullptr;
+    long long launches0 = launch_counter().load();
     VFS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
     try {
       fused_solve_direct(pairs, masked, half, st, variants, false);
@@ -418,6 +419,8 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
       throw;
     }
     prof->capture_events = nullptr;
+    e.kernels = launch_counter().load() - launches0;
+    launch_counter().fetch_sub(e.kernels);  // captured, not launched: counted when replayed
     VFS_CUDA(cudaStreamEndCapture(st, &g));
     cudaError_t ie = cudaGraphInstantiate(&e.exec, g, 0);
     cudaGraphDestroy(g);
@@ -429,6 +432,7 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     it = cache_.emplace(key, std::move(e)).first;
   }
   VFS_CUDA(cudaGraphLaunch(it->second.exec, st));
+  launch_counter().fetch_add(it->second.kernels);
   for (size_t k = 0; k < pairs.size(); k++) set_ptrs(pairs[k], it->second.after[k]);
   if (prof->profiling) prof->setProfRecords(it->second.prof);
 }

@@ -56,6 +56,7 @@ class FusedEngine {
  private:
   struct Entry {
     cudaGraphExec_t exec = nullptr;
+    long long kernels = 0;  // kernel launches recorded in the graph (added to the launch count per replay)
     std::vector<PairPtrs> after;
     std::vector<ProfRec> prof;
     std::vector<cudaEvent_t> events;
