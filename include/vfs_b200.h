@@ -142,6 +142,15 @@ int vfs_batch_solve(vfs_batch* b, int masked);
  * the variants on the first solve of each batch composition (on by default); the timing
  * launches do not change results.  Off: the default 31 x 8 tiles everywhere. */
 int vfs_batch_set_autotune(vfs_batch* b, int on);
+/* How a batch runs its pairs:
+ *   VFS_BATCH_CONCURRENT (default): each pair replays its own CUDA graph of one-pair fused
+ *     kernels on one of the batch's internal streams; the pairs run concurrently.
+ *   VFS_BATCH_ONE_LAUNCH: one launch per step and pyramid level covers every pair (the pair
+ *     is found per block from the launch's tile ranges).
+ * Both give identical results; concurrent graphs measure faster on B200. */
+#define VFS_BATCH_CONCURRENT 0
+#define VFS_BATCH_ONE_LAUNCH 1
+int vfs_batch_set_mode(vfs_batch* b, int mode);
 int vfs_set_autotune(vfs_stereo* s, int on);
 
 /* Histogram equalisation of n 8-bit pixels in device memory (d_dst may equal d_src), as
@@ -178,6 +187,16 @@ int vfs_profile_enable(vfs_stereo* s, int on);
 int vfs_profile_reset(vfs_stereo* s);
 int vfs_profile_read(vfs_stereo* s, int kind, long long* launches, double* total_ms,
                      double* pixel_iterations);
+/* vfs_profile_epoch() records one process-wide reference event on a stream (NULL: the
+ * legacy default stream).  vfs_profile_intervals() then returns, for the handle's records
+ * of a kind, their start and end in ms after that event and their pixel-iterations (up
+ * to max_records of them; *count receives the number of records).  Records of handles
+ * solved concurrently on different streams overlap; their union is the time during which
+ * at least one such group ran.  A graph replay re-records the events captured with it, so
+ * after several replays the records describe the last one. */
+int vfs_profile_epoch(void* cuda_stream);
+int vfs_profile_intervals(vfs_stereo* s, int kind, int max_records, double* start_ms, double* end_ms,
+                          double* pixel_iterations, int* count);
 
 /* ---- reference DLL entry points (dllhook/vfs.h:37-44) -------------------------------
  * Create / Init / SolveStereo with the reference's names and argument lists.  Init reads

@@ -65,12 +65,14 @@ def test_fused_odd_iteration_count(gpu):
         assert np.array_equal(a.debug_buffer(name, comps), b.debug_buffer(name, comps)), name
 
 
-def test_batch_uneven_sizes_bit_identical(gpu):
+@pytest.mark.parametrize("one_launch", [False, True])
+def test_batch_uneven_sizes_bit_identical(gpu, one_launch):
     from vfs_b200.stereotgv import StereoBatch
     cases = [(96, 64, 2), (130, 101, 3), (67, 53, 2), (200, 120, 3)]
     p0 = params(n_warp=2, n_iter=6)
     singles, members, data = [], [], []
     batch = StereoBatch()
+    batch.set_mode(one_launch)
     for k, (w, h, L) in enumerate(cases):
         i0, i1, mask, tv, cv = random_case(w, h, seed=100 + k)
         p = dict(p0, n_levels=L, alpha0=17.0 + k, limit_range=0.1 + 0.05 * k)

@@ -116,7 +116,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
       launch_level_tensor(L, st);
     }
     for (int warpIter = 0; warpIter < P0.nWarpIters; warpIter++) {
-      prof->profBeginPx(kProfPrologue, px_level, 1);
+      prof->profBeginPx(kProfPrologue, px_level, 1, st);
       {
         WarpStartArgs W{};
         for (int k = 0; k < na; k++) {
@@ -158,7 +158,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         Dv.npairs = na;
         launch_derivatives_batched(Dv, st);
       }
-      prof->profEnd();
+      prof->profEnd(st);
       auto iter_args = [&](int variant, float sigma_, float tau_, float mu_, int write_tp) {
         IterArgs A{};
         A.sigma = sigma_;
@@ -233,7 +233,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
       const int variant = level_variant[level] < 0 ? kIterDefaultVariant : level_variant[level];
       float tau = 1.0f;
       float sigma = 1.0f / tau;
-      prof->profBeginPx(kProfFused, px_level, P0.nSolverIters);
+      prof->profBeginPx(kProfFused, px_level, P0.nSolverIters, st);
       for (int iter = 0; iter < P0.nSolverIters; iter++) {
         float mu;
         if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P0.timestep_lambda);
@@ -250,8 +250,8 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         sigma = sigma / mu;
         tau = tau * mu;
       }
-      prof->profEnd();
-      prof->profBeginPx(kProfEpilogue, px_level, 1);
+      prof->profEnd(st);
+      prof->profBeginPx(kProfEpilogue, px_level, 1, st);
       {
         EpiArgs E{};
         E.median = masked ? 1 : 0;
@@ -275,7 +275,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         if (masked)
           for (auto* s : act) std::swap(s->d_u, s->d_us);
       }
-      prof->profEnd();
+      prof->profEnd(st);
     }
     if (level > 0) {
       UpArgs U{};

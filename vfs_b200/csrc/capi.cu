@@ -17,13 +17,20 @@ struct vfs_batch {
   cudaStream_t stream = 0;      // the batch's stream (its own unless set)
   cudaStream_t own = nullptr;
   cudaEvent_t done = nullptr;   // batch work finished (members' streams wait on it)
+  cudaEvent_t start = nullptr;  // members' inputs ready (the concurrent streams wait on it)
   std::vector<cudaEvent_t> ready;  // member work finished (the batch stream waits on them)
+  std::vector<cudaStream_t> lanes;     // concurrent mode: one stream per member slot
+  std::vector<cudaEvent_t> lane_done;  // concurrent mode: per-slot completion
+  int mode = VFS_BATCH_CONCURRENT;
   bool half = false;
   std::string err;
   ~vfs_batch() {
     engine.clear();
     for (auto e : ready) cudaEventDestroy(e);
+    for (auto e : lane_done) cudaEventDestroy(e);
+    for (auto l : lanes) cudaStreamDestroy(l);
     if (done) cudaEventDestroy(done);
+    if (start) cudaEventDestroy(start);
     if (own) cudaStreamDestroy(own);
   }
 };
@@ -335,6 +342,13 @@ int vfs_set_autotune(vfs_stereo* s, int on) {
   return guarded(s, [&] { s->impl.engine.autotune = on != 0; });
 }
 
+int vfs_batch_set_mode(vfs_batch* b, int mode) {
+  return guarded(b, [&] {
+    if (mode != VFS_BATCH_CONCURRENT && mode != VFS_BATCH_ONE_LAUNCH) throw vfs::ArgError{"unknown batch mode"};
+    b->mode = mode;
+  });
+}
+
 int vfs_batch_solve(vfs_batch* b, int masked) {
   return guarded(b, [&] {
     if (b->members.empty()) throw vfs::ArgError{"batch solve: empty batch"};
@@ -349,7 +363,40 @@ int vfs_batch_solve(vfs_batch* b, int masked) {
       VFS_CUDA(cudaEventRecord(b->ready[k], pairs[k]->stream()));
       VFS_CUDA(cudaStreamWaitEvent(b->stream, b->ready[k], 0));
     }
-    b->engine.solve(pairs, masked != 0, b->half, b->stream);
+    if (b->mode == VFS_BATCH_ONE_LAUNCH) {
+      b->engine.solve(pairs, masked != 0, b->half, b->stream);
+    } else {
+      // fork: every pair's solve (its own graph) on its own slot stream, then join
+      if (!b->start) VFS_CUDA(cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming));
+      while (b->lanes.size() < pairs.size()) {
+        cudaStream_t l;
+        VFS_CUDA(cudaStreamCreateWithFlags(&l, cudaStreamNonBlocking));
+        b->lanes.push_back(l);
+        cudaEvent_t e;
+        VFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->lane_done.push_back(e);
+      }
+      VFS_CUDA(cudaEventRecord(b->start, b->stream));
+      for (size_t k = 0; k < pairs.size(); k++) {
+        VFS_CUDA(cudaStreamWaitEvent(b->lanes[k], b->start, 0));
+        std::vector<vfs::StereoTgvImpl*> one{pairs[k]};
+        vfs::FusedEngine& eng = pairs[k]->engine;
+        const bool g = eng.use_graph, t = eng.autotune;
+        eng.use_graph = b->engine.use_graph;
+        eng.autotune = b->engine.autotune;
+        try {
+          eng.solve(one, masked != 0, b->half, b->lanes[k]);
+        } catch (...) {
+          eng.use_graph = g;
+          eng.autotune = t;
+          throw;
+        }
+        eng.use_graph = g;
+        eng.autotune = t;
+        VFS_CUDA(cudaEventRecord(b->lane_done[k], b->lanes[k]));
+        VFS_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
+      }
+    }
     VFS_CUDA(cudaEventRecord(b->done, b->stream));
     for (auto* p : pairs)
       if (p->stream() != b->stream) VFS_CUDA(cudaStreamWaitEvent(p->stream(), b->done, 0));
@@ -398,6 +445,47 @@ int vfs_profile_read(vfs_stereo* s, int kind, long long* n, double* ms, double* 
   return guarded(s, [&] {
     if (kind < 0 || kind >= vfs::kProfTags) throw vfs::ArgError{"profile kind out of range"};
     s->impl.profRead(kind, n, ms, pi);
+  });
+}
+
+// One process-wide reference event, so that records of different handles (solved on
+// different streams) can be placed on one time axis.
+static cudaEvent_t g_prof_epoch = nullptr;
+
+int vfs_profile_epoch(void* cuda_stream) {
+  cudaError_t e = cudaSuccess;
+  if (!g_prof_epoch) e = cudaEventCreate(&g_prof_epoch);
+  if (e == cudaSuccess) e = cudaEventRecord(g_prof_epoch, (cudaStream_t)cuda_stream);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    vfs::set_global_error(cudaGetErrorString(e));
+    return VFS_ERR_CUDA;
+  }
+  return VFS_OK;
+}
+
+int vfs_profile_intervals(vfs_stereo* s, int kind, int max_records, double* start_ms, double* end_ms,
+                          double* pixel_iterations, int* count) {
+  return guarded(s, [&] {
+    if (kind < 0 || kind >= vfs::kProfTags) throw vfs::ArgError{"profile kind out of range"};
+    if (!g_prof_epoch) throw vfs::ArgError{"vfs_profile_epoch() has not been recorded"};
+    if (max_records < 0 || !count) throw vfs::ArgError{"invalid output"};
+    VFS_CUDA(cudaEventSynchronize(g_prof_epoch));
+    int n = 0;
+    for (const auto& r : s->impl.profRecords()) {
+      if (r.tag != kind) continue;
+      if (n < max_records) {
+        VFS_CUDA(cudaEventSynchronize(r.b));
+        float a = 0, b = 0;
+        VFS_CUDA(cudaEventElapsedTime(&a, g_prof_epoch, r.a));
+        VFS_CUDA(cudaEventElapsedTime(&b, g_prof_epoch, r.b));
+        if (start_ms) start_ms[n] = a;
+        if (end_ms) end_ms[n] = b;
+        if (pixel_iterations) pixel_iterations[n] = (double)r.px * r.iters;
+      }
+      n++;
+    }
+    *count = n;
   });
 }
 

@@ -3,6 +3,9 @@
 #include "fused.cuh"
 #include "tgv_math.cuh"
 #include "tgv_pixel.cuh"
+#include "tgv_pixel_fast.cuh"
+
+#include <type_traits>
 
 namespace vfs {
 
@@ -36,16 +39,18 @@ struct FusedIter {
   typedef Store2<ST> S;
   typedef typename S::T2 T2;
   typedef typename S::T4 T4;
+  // Half storage takes the fused multiply-add / approximate reciprocal arithmetic of
+  // tgv_pixel_fast.cuh; float storage the exact forms of tgv_pixel.cuh.
+  static constexpr bool kFast = !std::is_same<ST, float>::value;
 
-  // dual update at an in-image pixel; returns false where the pixel keeps its
-  // values (masked out), in which case tp is the stored (stale) T p.
+  // dual update at an in-image pixel whose code and tensor are given; returns false where
+  // the pixel keeps its values (masked out), in which case tp is the stored (stale) T p.
+  // u_pos and vp (u-bar and v-bar here) are returned for the threshold and primal steps.
   static __device__ __forceinline__ bool dual_at(const IterPair& P, const T2* pin, const T4* qin, int ix, int iy,
-                                                 float sp, float sq, float2& p, float4& q, float2& tp) {
-    int pos = ix + iy * P.s;
+                                                 int pos, uint8_t code, float a, float b, float c, float sp, float sq,
+                                                 float& u_pos, float2& vp, float2& p, float4& q, float2& tp) {
     int right = pos + 1, down = pos + P.s, left = pos - 1, up = pos - P.s;
     bool useRight, useDown;
-    uint8_t code = P.code[pos];
-    float a = P.a[pos], b = P.b[pos], c = P.c[pos];
     if (MASKED) {
       if (!(code & kOn)) {
         tp = P.Tp[pos];
@@ -64,16 +69,21 @@ struct FusedIter {
       useDown = (iy + 1) < P.h;
     }
     const T2* v_ = (const T2*)P.v_;
-    float u_pos = P.u_[pos];
-    float2 vp = S::ld2(v_, pos);
+    u_pos = P.u_[pos];
+    vp = S::ld2(v_, pos);
     float u_xn = useRight ? P.u_[right] : (left < 0 ? 0.0f : P.u_[left]);
     float u_yn = useDown ? P.u_[down] : (up < 0 ? 0.0f : P.u_[up]);
     float2 v_xn = useRight ? S::ld2(v_, right) : (left < 0 ? make_float2(0.f, 0.f) : S::ld2(v_, left));
     float2 v_yn = useDown ? S::ld2(v_, down) : (up < 0 ? make_float2(0.f, 0.f) : S::ld2(v_, up));
     p = S::ld2(pin, pos);
     q = S::ld4(qin, pos);
-    dual_math(useRight, useDown, u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
-    tp = tp_math(a, b, c, p);
+    if (kFast) {
+      fast::dual(useRight, useDown, u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
+      tp = fast::tp(a, b, c, p);
+    } else {
+      dual_math(useRight, useDown, u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
+      tp = tp_math(a, b, c, p);
+    }
     return true;
   }
 };
@@ -82,17 +92,21 @@ struct FusedIter {
 // column and the first row being the halo of the 31 x TH tile.  Every thread
 // evaluates the dual update at its region pixel; after a barrier the tile threads
 // finish the threshold and primal steps with the west / north values from shared
-// memory.
-template <bool MASKED, class ST, int TH, int MINB>
+// memory.  The pixel's code, tensor, u-bar and v-bar stay in registers across the
+// barrier (no buffer the launch writes aliases them).
+// SINGLE: the launch carries one pair, whose descriptor fields then sit at fixed
+// parameter offsets (no per-block indexing of the parameter array).
+template <bool MASKED, class ST, int TH, int MINB, bool SINGLE>
 __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid_constant__ IterArgs A, int parity) {
   typedef FusedIter<MASKED, ST> F;
   typedef typename F::T2 T2;
   typedef typename F::T4 T4;
   typedef Store2<ST> S;
+  constexpr bool kFast = F::kFast;
   __shared__ float2 sTp[TH + 1][32];
   __shared__ float4 sQ[TH + 1][32];
   const int t_ = blockIdx.x;
-  const int pi_ = find_pair(A.pr, A.npairs, t_);
+  const int pi_ = SINGLE ? 0 : find_pair(A.pr, A.npairs, t_);
   const IterPair& P = A.pr[pi_];
   const int lt_ = t_ - P.tile0;
   const int x0 = (lt_ % P.tiles_x) * 31;
@@ -109,10 +123,16 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   const int pos = ix + iy * P.s;
 
   // ---- phase 1: dual update at every region pixel ------------------------------------
-  float2 pp = make_float2(0.f, 0.f), tp = make_float2(0.f, 0.f);
+  float2 pp = make_float2(0.f, 0.f), tp = make_float2(0.f, 0.f), vb = make_float2(0.f, 0.f);
   float4 qq = make_float4(0.f, 0.f, 0.f, 0.f);
+  uint8_t code = 0;
+  float a = 0.f, b = 0.f, c = 0.f, ubar = 0.f;
   if (in_img) {
-    bool own = F::dual_at(P, pin, qin, ix, iy, A.sp[pi_], A.sq[pi_], pp, qq, tp);
+    code = P.code[pos];
+    a = P.a[pos];
+    b = P.b[pos];
+    c = P.c[pos];
+    bool own = F::dual_at(P, pin, qin, ix, iy, pos, code, a, b, c, A.sp[pi_], A.sq[pi_], ubar, vb, pp, qq, tp);
     if (own && tile) {
       S::st2(pout, pos, pp);
       S::st4(qout, pos, qq);
@@ -129,8 +149,6 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   sQ[ry][rx] = qq;
   __syncthreads();
   if (!tile || !in_img) return;
-  uint8_t code = P.code[pos];
-  float a = P.a[pos], b = P.b[pos], c = P.c[pos];
 
   // ---- phase 2: thresholding --------------------------------------------------------
   float dxm, dym;
@@ -166,9 +184,14 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
     hasL = (ix - 1) >= 0;
     hasU = (iy - 1) >= 0;
   }
-  float ubar = P.u_[pos];
-  float eu = etau_math(a, b, c, P.alpha1);
-  float unew = threshold_math(dxm, dym, eu, A.tau, ubar, P.u[pos], P.Iu[pos], P.Iz[pos], P.lambda);
+  float unew;
+  if (kFast) {
+    float eu = fast::etau(a, b, c, P.alpha1 * P.alpha1);
+    unew = fast::threshold(dxm, dym, eu, A.tau, ubar, P.u[pos], P.Iu[pos], P.Iz[pos], P.lambda);
+  } else {
+    float eu = etau_math(a, b, c, P.alpha1);
+    unew = threshold_math(dxm, dym, eu, A.tau, ubar, P.u[pos], P.Iu[pos], P.Iz[pos], P.lambda);
+  }
   P.us[pos] = unew;
 
   // ---- phase 3: primal update ------------------------------------------------------
@@ -177,25 +200,37 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   if (zD) qc.y = qc.z = 0.0f;
   float4 ql = hasL ? sQ[ry][rx - 1] : make_float4(0.f, 0.f, 0.f, 0.f);
   float4 qu = hasU ? sQ[ry - 1][rx] : make_float4(0.f, 0.f, 0.f, 0.f);
-  float ev1 = etav1_math(b, c, P.alpha0, P.alpha1), ev2 = etav2_math(a, c, P.alpha0, P.alpha1);
-  float2 vb = S::ld2((const T2*)P.v_, pos);
   float us_;
-  float2 vs, vo;
-  primal_math(qc, ql, qu, pp, a, b, c, ev1, ev2, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs, vo);
+  float2 vs;
+  if (kFast) {
+    const float a1s = P.alpha1 * P.alpha1, a0s4 = 4.0f * P.alpha0 * P.alpha0;
+    float ev1 = fast::etav(b, c, a1s, a0s4), ev2 = fast::etav(a, c, a1s, a0s4);
+    fast::primal(qc, ql, qu, tp, ev1, ev2, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs);
+  } else {
+    float ev1 = etav1_math(b, c, P.alpha0, P.alpha1), ev2 = etav2_math(a, c, P.alpha0, P.alpha1);
+    float2 vo;
+    primal_math(qc, ql, qu, pp, a, b, c, ev1, ev2, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs, vo);
+  }
   P.u_s[pos] = us_;
   S::st2((T2*)P.v_s, pos, vs);
 }
 
-template <int TH, int MINB>
-static void launch_iter_th(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity) {
+template <int TH, int MINB, bool SINGLE>
+static void launch_iter_th2(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity) {
   dim3 blk(32, TH + 1);
   if (masked) {
-    if (half_storage) k_fused_iter<true, __half, TH, MINB><<<A.ntiles, blk, 0, st>>>(A, parity);
-    else k_fused_iter<true, float, TH, MINB><<<A.ntiles, blk, 0, st>>>(A, parity);
+    if (half_storage) k_fused_iter<true, __half, TH, MINB, SINGLE><<<A.ntiles, blk, 0, st>>>(A, parity);
+    else k_fused_iter<true, float, TH, MINB, SINGLE><<<A.ntiles, blk, 0, st>>>(A, parity);
   } else {
-    if (half_storage) k_fused_iter<false, __half, TH, MINB><<<A.ntiles, blk, 0, st>>>(A, parity);
-    else k_fused_iter<false, float, TH, MINB><<<A.ntiles, blk, 0, st>>>(A, parity);
+    if (half_storage) k_fused_iter<false, __half, TH, MINB, SINGLE><<<A.ntiles, blk, 0, st>>>(A, parity);
+    else k_fused_iter<false, float, TH, MINB, SINGLE><<<A.ntiles, blk, 0, st>>>(A, parity);
   }
+}
+
+template <int TH, int MINB>
+static void launch_iter_th(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity) {
+  if (A.npairs == 1) launch_iter_th2<TH, MINB, true>(A, masked, half_storage, st, parity);
+  else launch_iter_th2<TH, MINB, false>(A, masked, half_storage, st, parity);
 }
 
 void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,

@@ -49,16 +49,16 @@ void StereoTgvImpl::profBegin(int tag, int level, int iters) {
   profBeginPx(tag, (long long)pW[level] * pH[level], iters);
 }
 
-void StereoTgvImpl::profBeginPx(int tag, long long px, int iters) {
+void StereoTgvImpl::profBeginPx(int tag, long long px, int iters, cudaStream_t st) {
   if (!profiling) return;
   ProfRec r{tag, 0, px, iters, profEvent(), profEvent()};
-  record(r.a, stream_, capture_events != nullptr);
+  record(r.a, st ? st : stream_, capture_events != nullptr);
   prof_.push_back(r);
 }
 
-void StereoTgvImpl::profEnd() {
+void StereoTgvImpl::profEnd(cudaStream_t st) {
   if (!profiling || prof_.empty()) return;
-  record(prof_.back().b, stream_, capture_events != nullptr);
+  record(prof_.back().b, st ? st : stream_, capture_events != nullptr);
 }
 
 void StereoTgvImpl::profReset() {
@@ -68,6 +68,7 @@ void StereoTgvImpl::profReset() {
 
 void StereoTgvImpl::profRead(int tag, long long* count, double* total_ms, double* pixel_iters) {
   VFS_CUDA(cudaStreamSynchronize(stream_));
+  for (auto& r : prof_) VFS_CUDA(cudaEventSynchronize(r.b));  // records may sit on other streams
   long long n = 0;
   double t = 0, pi = 0;
   for (auto& r : prof_) {

@@ -168,8 +168,9 @@ class StereoTgvImpl {
  public:
   cudaEvent_t profEvent();
   void profBegin(int tag, int level, int iters);
-  void profBeginPx(int tag, long long px, int iters);
-  void profEnd();
+  // st: the stream the timed work is queued on (the handle's stream when 0)
+  void profBeginPx(int tag, long long px, int iters, cudaStream_t st = 0);
+  void profEnd(cudaStream_t st = 0);
 
  private:
   std::vector<ProfRec> prof_;

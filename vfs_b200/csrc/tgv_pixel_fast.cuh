@@ -1,0 +1,125 @@
+// Per-pixel arithmetic of the half-storage fused iteration.
+//
+// The same update as tgv_pixel.cuh (updateDualVariables.cu:33-98, thresholdingL1.cu:45-115,
+// updatePrimalVariables.cu:77-110, preconditioning.cu:18-20), evaluated with fused
+// multiply-adds and with the PTX instructions rcp.approx.ftz.f32 and rsqrt.approx.ftz.f32
+// (relative error below 2^-22) in place of IEEE division and square root.  On this path p,
+// q and v-bar are stored in half precision (relative rounding 2^-11), which dominates the
+// difference; the result is checked against the FP64 oracle with a tolerance.  The FP32
+// fused path keeps the exact forms of tgv_pixel.cuh and stays bit-identical to the drop-in
+// kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace vfs {
+namespace fast {
+
+__device__ __forceinline__ float rcp(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+__device__ __forceinline__ float rsqrt(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// Dual update.  A forward difference (right / down neighbour) and a backward one (left /
+// up) differ only in sign, so each is written as sgn * (neighbour - centre); the sign
+// change is exact.  The projection onto the unit ball multiplies by 1 / |p| where |p| > 1
+// (a NaN norm propagates, as max(rep, 1) does in the reference).
+__device__ __forceinline__ void dual(bool useRight, bool useDown, float u_pos, float u_xn, float u_yn, float2 vp,
+                                     float2 v_xn, float2 v_yn, float a, float b, float c, float sp, float sq,
+                                     float2& p, float4& q) {
+  const float sx = useRight ? 1.0f : -1.0f;
+  const float sy = useDown ? 1.0f : -1.0f;
+  float u_x = __fmaf_rn(sx, u_xn - u_pos, -vp.x);
+  float u_y = __fmaf_rn(sy, u_yn - u_pos, -vp.y);
+  float dtx = __fmaf_rn(a, u_x, c * u_y);
+  float dty = __fmaf_rn(c, u_x, b * u_y);
+  float ppx = __fmaf_rn(sp, dtx, p.x);
+  float ppy = __fmaf_rn(sp, dty, p.y);
+  float n2 = __fmaf_rn(ppx, ppx, ppy * ppy);
+  if (!(n2 <= 1.0f)) {
+    float r = rsqrt(n2);
+    ppx *= r;
+    ppy *= r;
+  }
+  p = make_float2(ppx, ppy);
+  const float qsx = sq * sx, qsy = sq * sy;  // exact: a sign change
+  float qx = __fmaf_rn(qsx, v_xn.x - vp.x, q.x);
+  float qy = __fmaf_rn(qsy, v_yn.y - vp.y, q.y);
+  float qz = __fmaf_rn(qsy, v_yn.x - vp.x, q.z);
+  float qw = __fmaf_rn(qsx, v_xn.y - vp.y, q.w);
+  float m2 = __fmaf_rn(qx, qx, __fmaf_rn(qy, qy, __fmaf_rn(qz, qz, qw * qw)));
+  if (!(m2 <= 1.0f)) {
+    float r = rsqrt(m2);
+    qx *= r;
+    qy *= r;
+    qz *= r;
+    qw *= r;
+  }
+  q = make_float4(qx, qy, qz, qw);
+}
+
+__device__ __forceinline__ float2 tp(float a, float b, float c, float2 p) {
+  return make_float2(__fmaf_rn(a, p.x, c * p.y), __fmaf_rn(c, p.x, b * p.y));
+}
+
+// Preconditioners eta_u, eta_v1, eta_v2 (a1s = alpha1^2, a0s4 = 4 alpha0^2).
+__device__ __forceinline__ float etau(float a, float b, float c, float a1s) {
+  float ac = a + c, bc = b + c;
+  float s = __fmaf_rn(a, a, b * b);
+  s = __fmaf_rn(2.0f * c, c, s);
+  s = __fmaf_rn(ac, ac, s);
+  s = __fmaf_rn(bc, bc, s);
+  return s * a1s;
+}
+__device__ __forceinline__ float etav(float x, float c, float a1s, float a0s4) {
+  return __fmaf_rn(a1s, __fmaf_rn(x, x, c * c), a0s4);
+}
+
+// L1 thresholding (the three cases of the linearised data term).
+__device__ __forceinline__ float threshold(float dxm, float dym, float eu, float tau, float u_bar, float upos,
+                                           float Ius, float Iz, float lambda) {
+  float div_p = dxm + dym;
+  float teu = (eu == 0.0f) ? tau : tau * rcp(eu);
+  float dun = __fmaf_rn(teu, div_p, u_bar) - upos;
+  float rho = __fmaf_rn(Ius, dun, Iz);
+  float lt = lambda * teu;
+  float upper = lt * (Ius * Ius);
+  float d = 0.0f;
+  if ((rho <= upper) && (rho >= -upper)) {
+    d = (Ius == 0.0f) ? dun : __fmaf_rn(-rho, rcp(Ius), dun);
+  } else if (rho < -upper) {
+    d = __fmaf_rn(lt, Ius, dun);
+  } else if (rho > upper) {
+    d = __fmaf_rn(-lt, Ius, dun);
+  }
+  return upos + d;
+}
+
+// Primal update of v and the over-relaxation of u and v; tpp = T p at this pixel.
+__device__ __forceinline__ void primal(float4 qc, float4 ql, float4 qu, float2 tpp, float ev1, float ev2, float tau,
+                                       float alpha0, float alpha1, float mu, float2 vb, float u_new, float u_bar,
+                                       float& u_s, float2& v_s) {
+  float dqx = (qc.x - ql.x) + (qc.z - qu.z);
+  float dqy = (qc.w - ql.w) + (qc.y - qu.y);
+  float gx = __fmaf_rn(alpha1, tpp.x, alpha0 * dqx);
+  float gy = __fmaf_rn(alpha1, tpp.y, alpha0 * dqy);
+  float vx, vy;
+  if (ev2 != 0.0f) {
+    vx = __fmaf_rn(ev1 != 0.0f ? tau * rcp(ev1) : tau, gx, vb.x);
+    vy = __fmaf_rn(tau * rcp(ev2), gy, vb.y);
+  } else {  // updatePrimalVariables.cu:103-105 writes .x again; .y keeps the previous value
+    vx = __fmaf_rn(tau, gx, vb.x);
+    vy = vb.y;
+  }
+  u_s = __fmaf_rn(mu, u_new - u_bar, u_new);
+  v_s = make_float2(__fmaf_rn(mu, vx - vb.x, vx), __fmaf_rn(mu, vy - vb.y, vy));
+}
+
+}  // namespace fast
+}  // namespace vfs

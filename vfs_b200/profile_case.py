@@ -1,11 +1,15 @@
 """A small, self-contained solve for profilers: one batched fused solve of `--batch` seeded
-848x800 pairs (no CUDA graph, so every kernel is an ordinary launch).
+848x800 pairs (no CUDA graph, so every kernel is an ordinary launch; no tile autotuning
+unless --autotune 1, so the launch sequence is fixed).
 
     python -m vfs_b200.profile_case --batch 4 --half 1 [--frames 1] [--path fused|plain]
+                                    [--mode concurrent|one_launch] [--autotune 0|1]
 
-Launch order per frame: pyramid, then per level (coarse to fine) the level kernels and
-per warp the prologue, the 50 fused iterations and the epilogue, so the first fused
-iteration at full resolution comes after 4 x 150 = 600 fused launches.
+Launch order per frame: pyramid, then per level (coarse to fine) the level kernels and per
+warp the prologue, the 50 fused iterations and the epilogue.  In the concurrent mode each
+pair's solve is enqueued in turn (pair 0 first), so k_fused_iter launches 600..749 are pair
+0's full-resolution iterations (one pair per launch).  In the one-launch mode every launch
+carries all pairs, and launches 600..749 are the full-resolution iterations of the batch.
 """
 from __future__ import annotations
 
@@ -23,6 +27,8 @@ def main():
     ap.add_argument("--path", default="fused", choices=["fused", "plain"])
     ap.add_argument("--width", type=int, default=848)
     ap.add_argument("--height", type=int, default=800)
+    ap.add_argument("--mode", default="concurrent", choices=["concurrent", "one_launch"])
+    ap.add_argument("--autotune", type=int, default=0)
     a = ap.parse_args()
     from . import synth
     from .stereotgv import StereoBatch, StereoTgv
@@ -39,6 +45,8 @@ def main():
     batch = StereoBatch(half_storage=bool(a.half)) if fused else None
     if batch is not None:
         batch.set_graph(False)
+        batch.set_autotune(bool(a.autotune))
+        batch.set_mode(one_launch=a.mode == "one_launch")
     solvers = []
     for _ in range(a.batch if fused else 1):
         s = StereoTgv()

@@ -25,6 +25,12 @@ def _ptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.c_void_p)
 
 
+def _stream_ptr(stream):
+    """cudaStream_t of a torch.cuda.Stream or a raw integer handle (None: the default stream)."""
+    raw = getattr(stream, "cuda_stream", stream)
+    return ctypes.c_void_p(int(raw) if raw else 0)
+
+
 class StereoTgv:
     """Variational fisheye stereo solver on one GPU (one camera pair)."""
 
@@ -209,6 +215,25 @@ class StereoTgv:
         check(self._h, self._L.vfs_profile_read(self._h, kind, ctypes.byref(n), ctypes.byref(ms), ctypes.byref(pi)))
         return n.value, ms.value, pi.value
 
+    @staticmethod
+    def profile_epoch(stream=None) -> None:
+        """Record the process-wide reference event of profile_intervals() on a stream."""
+        L = lib()
+        st = L.vfs_profile_epoch(_stream_ptr(stream))
+        if st != 0:
+            raise VfsError(st, L.vfs_last_error(None).decode(errors="replace"))
+
+    def profile_intervals(self, kind: int) -> np.ndarray:
+        """(start_ms, end_ms, pixel_iterations) rows of the records of a kind, relative to
+        the last profile_epoch()."""
+        n = ctypes.c_int()
+        check(self._h, self._L.vfs_profile_intervals(self._h, kind, 0, None, None, None, ctypes.byref(n)))
+        out = np.zeros((3, n.value), np.float64)
+        if n.value:
+            check(self._h, self._L.vfs_profile_intervals(self._h, kind, n.value, _ptr(out[0]), _ptr(out[1]),
+                                                         _ptr(out[2]), ctypes.byref(n)))
+        return out.T.copy()
+
     def debug_buffer(self, name: str, comps: int = 1) -> np.ndarray:
         out = np.empty((self.height, self.width, comps), np.float32)
         check(self._h, self._L.vfs_debug_get_buffer(self._h, name.encode(), comps, _ptr(out)))
@@ -260,6 +285,11 @@ class StereoBatch:
 
     def set_autotune(self, on: bool) -> None:
         check_batch(self._h, self._L.vfs_batch_set_autotune(self._h, int(on)))
+
+    def set_mode(self, one_launch: bool) -> None:
+        """False (default): pairs run concurrently, each from its own CUDA graph; True: one
+        launch per step and level covers all pairs."""
+        check_batch(self._h, self._L.vfs_batch_set_mode(self._h, int(one_launch)))
 
     def add(self, solver: "StereoTgv") -> None:
         check_batch(self._h, self._L.vfs_batch_add(self._h, solver.handle))
