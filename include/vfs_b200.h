@@ -138,6 +138,16 @@ int vfs_batch_size(const vfs_batch* b);
 int vfs_batch_set_storage(vfs_batch* b, int half_storage);
 int vfs_batch_set_graph(vfs_batch* b, int use_graph);
 int vfs_batch_solve(vfs_batch* b, int masked);
+/* One batched solve from and to host memory: the reference's per-frame sequence
+ * copyImagesToDevice(uchar*, uchar*) -> solveStereoForward[Masked] -> copy1DDisparityToHost
+ * (stereotgv.cu:201-213, 256-515, 533-540) for every pair of the batch in one call.  Pair k
+ * reads its tight W x H u8 images from i0[k] and i1[k] and writes its tight W x H float32
+ * disparity to u_out[k].  Each pair's upload, solve and download are queued on that pair's
+ * lane, so the copies of one pair overlap the solves of the others.  Returns when every
+ * output is in host memory.  Page-locked host buffers are copied asynchronously by the copy
+ * engines; pageable ones work but are staged by the driver. */
+int vfs_batch_solve_host(vfs_batch* b, const uint8_t* const* i0, const uint8_t* const* i1,
+                         float* const* u_out, int masked);
 /* The fused path picks the tile height of its iteration kernel per pyramid level by timing
  * the variants on the first solve of each batch composition (on by default); the timing
  * launches do not change results.  Off: the default 31 x 8 tiles everywhere. */

@@ -107,3 +107,37 @@ def test_half_storage_accuracy(gpu):
     d = np.abs(u.astype(np.float64) - o.get("u"))[m]
     assert d.mean() <= 0.05, d.mean()
     assert (d > 1.0).mean() < 0.01
+
+
+@pytest.mark.parametrize("one_launch", [False, True])
+def test_batch_solve_host_matches_device_path(gpu, one_launch):
+    """vfs_batch_solve_host (upload, solve and download per pair in one call) gives the same
+    disparities as the device-resident sequence copyImagesToDevice -> vfs_batch_solve ->
+    copy1DDisparityToHost, over two frames, from pageable and from page-locked buffers."""
+    import torch
+    from vfs_b200.stereotgv import StereoBatch
+    cases = [(96, 64, 2), (130, 101, 3), (67, 53, 2)]
+    p0 = params(n_warp=2, n_iter=6)
+    ref_batch, host_batch = StereoBatch(half_storage=True), StereoBatch(half_storage=True)
+    ref_batch.set_mode(one_launch)
+    host_batch.set_mode(one_launch)
+    data = []
+    for k, (w, h, L) in enumerate(cases):
+        i0, i1, mask, tv, cv = random_case(w, h, seed=300 + k)
+        p = dict(p0, n_levels=L)
+        ref_batch.add(make(i0, i1, mask, tv, cv, p, fused=True, half=True))
+        host_batch.add(make(i0, i1, mask, tv, cv, p, fused=True, half=True))
+        data.append((i0, i1))
+    pinned = [(torch.from_numpy(a).pin_memory(), torch.from_numpy(b).pin_memory()) for a, b in data]
+    outs = [torch.full((h, w), -1.0).pin_memory() for (w, h, _) in cases]
+    for frame in range(2):
+        for m, (i0, i1) in zip(ref_batch.members, data):
+            m.copyImagesToDevice(i0, i1)
+        ref_batch.solve(True)
+        want = [m.copy1DDisparityToHost() for m in ref_batch.members]
+        if frame == 0:
+            got = host_batch.solve_host(data)
+        else:
+            got = host_batch.solve_host([(a.numpy(), b.numpy()) for a, b in pinned], [o.numpy() for o in outs])
+        for k, (g, w_) in enumerate(zip(got, want)):
+            assert np.array_equal(np.asarray(g), w_), (frame, k)

@@ -73,6 +73,7 @@ SIGNATURES = {
     "vfs_batch_set_storage": [_vp, _i],
     "vfs_batch_set_graph": [_vp, _i],
     "vfs_batch_solve": [_vp, _i],
+    "vfs_batch_solve_host": [_vp, _vp, _vp, _vp, _i],
     "vfs_batch_set_autotune": [_vp, _i],
     "vfs_batch_set_mode": [_vp, _i],
     "vfs_set_autotune": [_vp, _i],

@@ -349,57 +349,97 @@ int vfs_batch_set_mode(vfs_batch* b, int mode) {
   });
 }
 
-int vfs_batch_solve(vfs_batch* b, int masked) {
-  return guarded(b, [&] {
-    if (b->members.empty()) throw vfs::ArgError{"batch solve: empty batch"};
-    std::vector<vfs::StereoTgvImpl*> pairs;
-    for (auto* m : b->members) pairs.push_back(&m->impl);
-    // per-pair preparation on each member's own stream, then order the batch stream
-    // after every member's queued work and every member's stream after the batch
-    vfs::FusedEngine::prepare(pairs, masked != 0);
-    if (!b->done) VFS_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
-    for (size_t k = 0; k < pairs.size(); k++) {
-      if (pairs[k]->stream() == b->stream) continue;
-      VFS_CUDA(cudaEventRecord(b->ready[k], pairs[k]->stream()));
-      VFS_CUDA(cudaStreamWaitEvent(b->stream, b->ready[k], 0));
+}  // extern "C"
+
+namespace {
+
+// Host buffers of a batched solve from and to host memory (null: device-resident inputs
+// already copied by the caller, outputs left on the device).
+struct BatchHostIO {
+  const uint8_t* const* i0 = nullptr;
+  const uint8_t* const* i1 = nullptr;
+  float* const* u = nullptr;
+};
+
+void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
+  if (b->members.empty()) throw vfs::ArgError{"batch solve: empty batch"};
+  std::vector<vfs::StereoTgvImpl*> pairs;
+  for (auto* m : b->members) pairs.push_back(&m->impl);
+  if (io) {
+    for (size_t k = 0; k < pairs.size(); k++)
+      if (!io->i0[k] || !io->i1[k] || !io->u[k]) throw vfs::ArgError{"batch solve: null host buffer"};
+  }
+  // per-pair preparation on each member's own stream, then order the batch stream
+  // after every member's queued work and every member's stream after the batch
+  vfs::FusedEngine::prepare(pairs, masked != 0);
+  if (!b->done) VFS_CUDA(cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming));
+  for (size_t k = 0; k < pairs.size(); k++) {
+    if (pairs[k]->stream() == b->stream) continue;
+    VFS_CUDA(cudaEventRecord(b->ready[k], pairs[k]->stream()));
+    VFS_CUDA(cudaStreamWaitEvent(b->stream, b->ready[k], 0));
+  }
+  if (b->mode == VFS_BATCH_ONE_LAUNCH) {
+    if (io)
+      for (size_t k = 0; k < pairs.size(); k++)
+        pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], cudaMemcpyHostToDevice, b->stream);
+    b->engine.solve(pairs, masked != 0, b->half, b->stream);
+    if (io)
+      for (size_t k = 0; k < pairs.size(); k++) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, b->stream);
+  } else {
+    // fork: every pair's upload, solve (its own graph) and download on its own slot
+    // stream, then join; one pair's copies overlap the other pairs' solves
+    if (!b->start) VFS_CUDA(cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming));
+    while (b->lanes.size() < pairs.size()) {
+      cudaStream_t l;
+      VFS_CUDA(cudaStreamCreateWithFlags(&l, cudaStreamNonBlocking));
+      b->lanes.push_back(l);
+      cudaEvent_t e;
+      VFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      b->lane_done.push_back(e);
     }
-    if (b->mode == VFS_BATCH_ONE_LAUNCH) {
-      b->engine.solve(pairs, masked != 0, b->half, b->stream);
-    } else {
-      // fork: every pair's solve (its own graph) on its own slot stream, then join
-      if (!b->start) VFS_CUDA(cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming));
-      while (b->lanes.size() < pairs.size()) {
-        cudaStream_t l;
-        VFS_CUDA(cudaStreamCreateWithFlags(&l, cudaStreamNonBlocking));
-        b->lanes.push_back(l);
-        cudaEvent_t e;
-        VFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-        b->lane_done.push_back(e);
-      }
-      VFS_CUDA(cudaEventRecord(b->start, b->stream));
-      for (size_t k = 0; k < pairs.size(); k++) {
-        VFS_CUDA(cudaStreamWaitEvent(b->lanes[k], b->start, 0));
-        std::vector<vfs::StereoTgvImpl*> one{pairs[k]};
-        vfs::FusedEngine& eng = pairs[k]->engine;
-        const bool g = eng.use_graph, t = eng.autotune;
-        eng.use_graph = b->engine.use_graph;
-        eng.autotune = b->engine.autotune;
-        try {
-          eng.solve(one, masked != 0, b->half, b->lanes[k]);
-        } catch (...) {
-          eng.use_graph = g;
-          eng.autotune = t;
-          throw;
-        }
+    VFS_CUDA(cudaEventRecord(b->start, b->stream));
+    for (size_t k = 0; k < pairs.size(); k++) {
+      VFS_CUDA(cudaStreamWaitEvent(b->lanes[k], b->start, 0));
+      if (io) pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], cudaMemcpyHostToDevice, b->lanes[k]);
+      std::vector<vfs::StereoTgvImpl*> one{pairs[k]};
+      vfs::FusedEngine& eng = pairs[k]->engine;
+      const bool g = eng.use_graph, t = eng.autotune;
+      eng.use_graph = b->engine.use_graph;
+      eng.autotune = b->engine.autotune;
+      try {
+        eng.solve(one, masked != 0, b->half, b->lanes[k]);
+      } catch (...) {
         eng.use_graph = g;
         eng.autotune = t;
-        VFS_CUDA(cudaEventRecord(b->lane_done[k], b->lanes[k]));
-        VFS_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
+        throw;
       }
+      eng.use_graph = g;
+      eng.autotune = t;
+      if (io) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, b->lanes[k]);
+      VFS_CUDA(cudaEventRecord(b->lane_done[k], b->lanes[k]));
+      VFS_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
     }
-    VFS_CUDA(cudaEventRecord(b->done, b->stream));
-    for (auto* p : pairs)
-      if (p->stream() != b->stream) VFS_CUDA(cudaStreamWaitEvent(p->stream(), b->done, 0));
+  }
+  VFS_CUDA(cudaEventRecord(b->done, b->stream));
+  for (auto* p : pairs)
+    if (p->stream() != b->stream) VFS_CUDA(cudaStreamWaitEvent(p->stream(), b->done, 0));
+  if (io) VFS_CUDA(cudaStreamSynchronize(b->stream));
+}
+
+}  // namespace
+
+extern "C" {
+
+int vfs_batch_solve(vfs_batch* b, int masked) {
+  return guarded(b, [&] { batch_solve(b, masked, nullptr); });
+}
+
+int vfs_batch_solve_host(vfs_batch* b, const uint8_t* const* i0, const uint8_t* const* i1, float* const* u_out,
+                         int masked) {
+  return guarded(b, [&] {
+    if (!i0 || !i1 || !u_out) throw vfs::ArgError{"batch solve: null host buffer list"};
+    BatchHostIO io{i0, i1, u_out};
+    batch_solve(b, masked, &io);
   });
 }
 

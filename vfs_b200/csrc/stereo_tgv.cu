@@ -276,14 +276,17 @@ void StereoTgvImpl::copyMaskToDevice(const float* mask) {
 
 // stereotgv.cu:201-213 (u8) and 215-239 (f32, u8c3)
 void StereoTgvImpl::copyImagesU8(const uint8_t* i0, const uint8_t* i1, bool device_src) {
+  copyImagesU8On(i0, i1, device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, stream_);
+  if (!device_src) VFS_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void StereoTgvImpl::copyImagesU8On(const uint8_t* i0, const uint8_t* i1, cudaMemcpyKind kind, cudaStream_t st) {
   if (!initialized_) throw ArgError{"copyImagesToDevice before initialize"};
   if (!i0 || !i1) throw ArgError{"copyImagesToDevice: null image"};
-  cudaMemcpyKind kind = device_src ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  VFS_CUDA(cudaMemcpy2DAsync(d_i08u, stride, i0, width, width, height, kind, stream_));
-  VFS_CUDA(cudaMemcpy2DAsync(d_i18u, stride, i1, width, width, height, kind, stream_));
-  launch_cv8u_to_gray(d_i08u, pI0[0], geom(0), stream_);
-  launch_cv8u_to_gray(d_i18u, pI1[0], geom(0), stream_);
-  if (!device_src) VFS_CUDA(cudaStreamSynchronize(stream_));
+  VFS_CUDA(cudaMemcpy2DAsync(d_i08u, stride, i0, width, width, height, kind, st));
+  VFS_CUDA(cudaMemcpy2DAsync(d_i18u, stride, i1, width, width, height, kind, st));
+  launch_cv8u_to_gray(d_i08u, pI0[0], geom(0), st);
+  launch_cv8u_to_gray(d_i18u, pI1[0], geom(0), st);
 }
 
 void StereoTgvImpl::copyImagesF32(const float* i0, const float* i1) {
@@ -431,6 +434,11 @@ void StereoTgvImpl::solveReference(bool masked) {
 
 // stereotgv.cu:517-568 outputs: level-0 views of u, warpUV, the warped image.
 void StereoTgvImpl::copyOut(const char* what, float* dst, bool to_host) {
+  copyOutOn(what, dst, to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, stream_);
+  if (to_host) VFS_CUDA(cudaStreamSynchronize(stream_));
+}
+
+void StereoTgvImpl::copyOutOn(const char* what, float* dst, cudaMemcpyKind kind, cudaStream_t st) {
   if (!initialized_) throw ArgError{"copy before initialize"};
   if (!dst) throw ArgError{"copy: null destination"};
   const void* src = nullptr;
@@ -443,9 +451,7 @@ void StereoTgvImpl::copyOut(const char* what, float* dst, bool to_host) {
   else if (!std::strcmp(what, "rgb")) { src = d_uvrgb; comps = 3; }
   else throw ArgError{std::string("copy: unknown buffer ") + what};
   size_t row = (size_t)width * comps * sizeof(float);
-  VFS_CUDA(cudaMemcpy2DAsync(dst, row, src, (size_t)stride * comps * sizeof(float), row, height,
-                             to_host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, stream_));
-  if (to_host) VFS_CUDA(cudaStreamSynchronize(stream_));
+  VFS_CUDA(cudaMemcpy2DAsync(dst, row, src, (size_t)stride * comps * sizeof(float), row, height, kind, st));
 }
 
 void StereoTgvImpl::convertKB(float fx, float fy, float cx, float cy, float d1, float d2, float d3, float d4, float t1_,

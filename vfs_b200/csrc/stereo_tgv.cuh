@@ -87,6 +87,9 @@ class StereoTgvImpl {
   void copyImagesU8C3(const uint8_t* i0, const uint8_t* i1);
   void solve(bool masked);
   void copyOut(const char* what, float* dst, bool to_host);
+  // stream-ordered forms on a given stream (no synchronisation): the batched host-buffer solve
+  void copyImagesU8On(const uint8_t* i0, const uint8_t* i1, cudaMemcpyKind kind, cudaStream_t st);
+  void copyOutOn(const char* what, float* dst, cudaMemcpyKind kind, cudaStream_t st);
   void convertKB(float fx, float fy, float cx, float cy, float d1, float d2, float d3, float d4, float t1, float t2,
                  float t3);
   void flowToHSV(float flowscale);

@@ -302,5 +302,29 @@ class StereoBatch:
     def solve(self, masked: bool = True) -> None:
         check_batch(self._h, self._L.vfs_batch_solve(self._h, int(masked)))
 
+    def solve_host(self, images, outputs=None, masked: bool = True):
+        """One solve of every pair from and to host memory: ``images[k] = (i0, i1)``, tight
+        H x W uint8 arrays of pair k; the disparities go to ``outputs[k]`` (H x W float32,
+        allocated when not given).  Page-locked arrays (e.g. from ``torch.pin_memory``)
+        are copied asynchronously.  Returns the outputs once they are in host memory."""
+        n = len(self.members)
+        if len(images) != n:
+            raise VfsError(-1, f"solve_host: {len(images)} image pairs for a batch of {n}")
+        if outputs is None:
+            outputs = [np.empty((m.height, m.width), np.float32) for m in self.members]
+        keep = []
+        for m, (a, b), o in zip(self.members, images, outputs):
+            for x, dt in ((a, np.uint8), (b, np.uint8), (o, np.float32)):
+                if not (isinstance(x, np.ndarray) and x.dtype == dt and x.flags.c_contiguous
+                        and x.shape == (m.height, m.width)):
+                    raise VfsError(-1, "solve_host: need contiguous H x W uint8 images and float32 outputs")
+            keep += [a, b, o]
+        P = ctypes.c_void_p * n
+        i0 = P(*[a.ctypes.data for a, _ in images])
+        i1 = P(*[b.ctypes.data for _, b in images])
+        uo = P(*[o.ctypes.data for o in outputs])
+        check_batch(self._h, self._L.vfs_batch_solve_host(self._h, i0, i1, uo, int(masked)))
+        return outputs
+
     def __len__(self):
         return len(self.members)
