@@ -162,6 +162,14 @@ int vfs_batch_set_autotune(vfs_batch* b, int on);
 #define VFS_BATCH_ONE_LAUNCH 1
 int vfs_batch_set_mode(vfs_batch* b, int mode);
 int vfs_set_autotune(vfs_stereo* s, int on);
+/* Force one variant of the fused iteration kernel at every pyramid level (-1: the tuned or
+ * default choice).  0-2: 32 x (4, 8, 16 + 1)-thread blocks exchanging the west / north
+ * neighbours' T p and q through shared memory; 3-5: one warp per 31-column strip of 8, 16
+ * or 32 rows, neighbours by warp shuffle and registers.  Every variant gives the same
+ * results; this selects speed only.  (No counterpart in the reference.) */
+#define VFS_ITER_VARIANTS 6
+int vfs_set_iteration_variant(vfs_stereo* s, int variant);
+int vfs_batch_set_iteration_variant(vfs_batch* b, int variant);
 
 /* Histogram equalisation of n 8-bit pixels in device memory (d_dst may equal d_src), as
  * cv::equalizeHist, which the reference's SolveStereo applies to both images on the host
@@ -193,6 +201,11 @@ int vfs_equalize_hist_u8_noalloc(const uint8_t* d_src, uint8_t* d_dst, size_t n,
  * vfs_profile_read() sums the records of a group kind (0 = drop-in inner iteration,
  * 1 = fused inner launch, 2 = fused per-warp prologue, 3 = fused epilogue). */
 long long vfs_launch_count(void);
+/* Process-wide: launch the fused iteration kernels with programmatic dependent launch
+ * (on = 1, the default), so that each launch is scheduled while the previous one drains;
+ * every such kernel waits for its predecessor's results before reading memory, so the
+ * results are the same either way.  Graphs captured before a change keep the old setting. */
+int vfs_set_launch_overlap(int on);
 int vfs_profile_enable(vfs_stereo* s, int on);
 int vfs_profile_reset(vfs_stereo* s);
 int vfs_profile_read(vfs_stereo* s, int kind, long long* launches, double* total_ms,

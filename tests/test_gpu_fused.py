@@ -141,3 +141,72 @@ def test_batch_solve_host_matches_device_path(gpu, one_launch):
             got = host_batch.solve_host([(a.numpy(), b.numpy()) for a, b in pinned], [o.numpy() for o in outs])
         for k, (g, w_) in enumerate(zip(got, want)):
             assert np.array_equal(np.asarray(g), w_), (frame, k)
+
+
+@pytest.mark.parametrize("masked", [True, False])
+def test_every_iteration_variant_bit_identical(gpu, masked):
+    """All variants of the fused iteration kernel (shared-memory tiles of 4 / 8 / 16 rows and
+    row-streaming strips of 8 / 16 / 32 rows) give the drop-in path's bits with float storage
+    and one another's bits with half storage, on sizes that cut strips and rows unevenly."""
+    from vfs_b200.stereotgv import StereoBatch
+    cases = [(97, 71, 2), (131, 45, 3), (40, 100, 2)]
+    p0 = params(n_warp=2, n_iter=7)
+    for k, (w, h, L) in enumerate(cases):
+        i0, i1, mask, tv, cv = random_case(w, h, seed=500 + k)
+        p = dict(p0, n_levels=L)
+        ref = make(i0, i1, mask, tv, cv, p, fused=False)
+        solve_frames(ref, i0, i1, masked, 2)
+        want = {n: ref.debug_buffer(n, c) for n, c in (("u", 1), ("u_", 1), ("warpUV", 2), ("Tp", 2))}
+        half_ref = None
+        for variant in range(6):
+            s = make(i0, i1, mask, tv, cv, p, fused=True)
+            s.set_iteration_variant(variant)
+            solve_frames(s, i0, i1, masked, 2)
+            for n, c in (("u", 1), ("u_", 1), ("warpUV", 2), ("Tp", 2)):
+                assert np.array_equal(s.debug_buffer(n, c), want[n]), (w, h, variant, n)
+            sh = make(i0, i1, mask, tv, cv, p, fused=True, half=True)
+            sh.set_iteration_variant(variant)
+            solve_frames(sh, i0, i1, masked, 2)
+            u = sh.copy1DDisparityToHost()
+            if half_ref is None:
+                half_ref = u
+            assert np.array_equal(u, half_ref), (w, h, variant, "half")
+    # batched one-launch form with a forced streaming variant
+    b = StereoBatch(half_storage=False)
+    b.set_mode(True)
+    b.set_iteration_variant(4)
+    members, singles, data = [], [], []
+    for k, (w, h, L) in enumerate(cases):
+        i0, i1, mask, tv, cv = random_case(w, h, seed=600 + k)
+        p = dict(p0, n_levels=L)
+        m = make(i0, i1, mask, tv, cv, p, fused=True)
+        b.add(m)
+        members.append(m)
+        singles.append(make(i0, i1, mask, tv, cv, p, fused=False))
+        data.append((i0, i1))
+    for m, (i0, i1) in zip(members, data):
+        m.copyImagesToDevice(i0, i1)
+    b.solve(masked)
+    for s, m, (i0, i1) in zip(singles, members, data):
+        solve_frames(s, i0, i1, masked, 1)
+        m.synchronize()
+        assert np.array_equal(s.debug_buffer("u", 1), m.debug_buffer("u", 1))
+
+
+def test_launch_overlap_does_not_change_results(gpu):
+    """Programmatic dependent launch of the iteration kernels (the default) and plain
+    stream-ordered launches give the same bits."""
+    from vfs_b200._native import lib
+    i0, i1, mask, tv, cv = random_case(150, 90, seed=77)
+    p = params(n_levels=3, n_warp=2, n_iter=9)
+    out = []
+    try:
+        for on in (1, 0):
+            assert lib().vfs_set_launch_overlap(on) == 0
+            for half in (False, True):
+                s = make(i0, i1, mask, tv, cv, p, fused=True, half=half)
+                solve_frames(s, i0, i1, True, 2)
+                out.append(s.copy1DDisparityToHost())
+    finally:
+        lib().vfs_set_launch_overlap(1)
+    assert np.array_equal(out[0], out[2]) and np.array_equal(out[1], out[3])

@@ -77,10 +77,13 @@ SIGNATURES = {
     "vfs_batch_set_autotune": [_vp, _i],
     "vfs_batch_set_mode": [_vp, _i],
     "vfs_set_autotune": [_vp, _i],
+    "vfs_set_iteration_variant": [_vp, _i],
+    "vfs_batch_set_iteration_variant": [_vp, _i],
     "vfs_equalize_hist_u8": [_vp, _vp, _sz, _vp],
     "vfs_equalize_hist_u8_noalloc": [_vp, _vp, _sz, _i, _vp],
     "vfs_estimate_device_bytes": [_i, _i, _i, _f, _i, _i],
     "vfs_launch_count": [],
+    "vfs_set_launch_overlap": [_i],
     "vfs_profile_enable": [_vp, _i],
     "vfs_profile_reset": [_vp],
     "vfs_profile_read": [_vp, _i, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),

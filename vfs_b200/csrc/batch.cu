@@ -368,6 +368,7 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   std::vector<int> comp{(int)masked, (int)half};
   for (auto& g : geo) comp.insert(comp.end(), g.begin(), g.end());
   auto tit = tuned_.find(comp);
+  if (tit == tuned_.end() && forced_variant >= 0) tit = tuned_.emplace(comp, std::vector<int>(maxL, forced_variant)).first;
   if (tit == tuned_.end()) {
     std::vector<int> lv(maxL, autotune ? -1 : kIterDefaultVariant);
     if (autotune) {
@@ -379,6 +380,7 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     tit = tuned_.emplace(comp, lv).first;
   }
   std::vector<int> variants = tit->second;
+  if (forced_variant >= 0) variants.assign(maxL, forced_variant);
   if (!use_graph) {
     fused_solve_direct(pairs, masked, half, st, variants, false);
     return;

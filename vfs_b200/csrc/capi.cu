@@ -342,6 +342,20 @@ int vfs_set_autotune(vfs_stereo* s, int on) {
   return guarded(s, [&] { s->impl.engine.autotune = on != 0; });
 }
 
+int vfs_set_iteration_variant(vfs_stereo* s, int variant) {
+  return guarded(s, [&] {
+    if (variant < -1 || variant >= vfs::kIterVariants) throw vfs::ArgError{"iteration variant out of range"};
+    s->impl.engine.forced_variant = variant;
+  });
+}
+
+int vfs_batch_set_iteration_variant(vfs_batch* b, int variant) {
+  return guarded(b, [&] {
+    if (variant < -1 || variant >= vfs::kIterVariants) throw vfs::ArgError{"iteration variant out of range"};
+    b->engine.forced_variant = variant;
+  });
+}
+
 int vfs_batch_set_mode(vfs_batch* b, int mode) {
   return guarded(b, [&] {
     if (mode != VFS_BATCH_CONCURRENT && mode != VFS_BATCH_ONE_LAUNCH) throw vfs::ArgError{"unknown batch mode"};
@@ -404,17 +418,21 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
       std::vector<vfs::StereoTgvImpl*> one{pairs[k]};
       vfs::FusedEngine& eng = pairs[k]->engine;
       const bool g = eng.use_graph, t = eng.autotune;
+      const int fv = eng.forced_variant;
       eng.use_graph = b->engine.use_graph;
       eng.autotune = b->engine.autotune;
+      eng.forced_variant = b->engine.forced_variant;
       try {
         eng.solve(one, masked != 0, b->half, b->lanes[k]);
       } catch (...) {
         eng.use_graph = g;
         eng.autotune = t;
+        eng.forced_variant = fv;
         throw;
       }
       eng.use_graph = g;
       eng.autotune = t;
+      eng.forced_variant = fv;
       if (io) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, b->lanes[k]);
       VFS_CUDA(cudaEventRecord(b->lane_done[k], b->lanes[k]));
       VFS_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
@@ -469,6 +487,11 @@ int vfs_equalize_hist_u8(const uint8_t* d_src, uint8_t* d_dst, size_t n, void* c
 }
 
 long long vfs_launch_count(void) { return vfs::launch_counter().load(); }
+
+int vfs_set_launch_overlap(int on) {
+  vfs::pdl_enabled().store(on != 0);
+  return VFS_OK;
+}
 
 int vfs_profile_enable(vfs_stereo* s, int on) {
   return guarded(s, [&] { s->impl.profiling = on != 0; });

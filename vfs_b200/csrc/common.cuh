@@ -48,6 +48,35 @@ struct ArgError {
   std::string msg;
 };
 
+// Programmatic dependent launch of the fused iteration kernels.  With it on, the next launch
+// on a stream may be scheduled while the previous one drains; every kernel launched this way
+// executes griddep_wait() before its first global-memory access, which returns once the
+// previous launch has completed and its writes are visible, so results do not depend on the
+// overlap.  Process-wide switch (vfs_set_launch_overlap), on by default.
+std::atomic<bool>& pdl_enabled();
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+template <typename... KArgs, typename... Args>
+inline void launch_overlapped(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+  if (!pdl_enabled().load(std::memory_order_relaxed)) {
+    k<<<grid, block, 0, st>>>(args...);
+    return;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  VFS_CUDA(cudaLaunchKernelEx(&cfg, k, args...));
+}
+
 inline int iDivUp(int n, int m) { return (n + m - 1) / m; }
 
 // Launch shape of the plain per-pixel kernels: 32 columns x 8 rows, so a warp reads

@@ -56,6 +56,14 @@ struct Store2<__half> {
   }
 };
 
+// Locate the pair that owns tile t from the batch's tile ranges.
+template <class PairT, int N>
+__device__ __forceinline__ int find_pair(const PairT (&pr)[N], int npairs, int t) {
+  int k = 0;
+  while (k + 1 < npairs && t >= pr[k + 1].tile0) k++;
+  return k;
+}
+
 // ---- one primal-dual iteration -------------------------------------------------
 struct IterPair {
   const uint8_t* code;  // edge codes (masked form) or inside-circle flags (plain form)
@@ -83,6 +91,9 @@ struct IterArgs {
 // variant selects the tile height (kIterVariantRows[variant] rows of 31 pixels).
 void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
                             int variant);
+// the row-streaming form with `rows` (8, 16 or 32) output rows per warp
+void launch_fused_iteration_rows(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
+                                 int rows);
 
 // ---- per-warp prologue: zero p, q, v-bar; resample tv at x + warpUV; warp I1 ----
 struct WarpStartPair {
@@ -188,9 +199,13 @@ inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFT
 // Tile-height variants of the iteration kernel (chosen per level by the autotuner in
 // FusedEngine): rows per tile and the minimum resident blocks per SM its launch bounds
 // ask for (which caps registers at 32 or 40 per thread).
-constexpr int kIterVariants = 3;
-constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16};
-constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3};
+// Variants 0-2: k_fused_iter (32 x (rows + 1) blocks, shared-memory west / north exchange);
+// variants 3-5: k_fused_iter_rows (one warp walks down a 31-column strip of `rows` rows,
+// neighbours by shuffle and registers; kernels_rows.cu).  All give identical results.
+constexpr int kIterVariants = 6;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0};
+constexpr int kIterFirstRowsVariant = 3;
 constexpr int kIterDefaultVariant = 1;
 inline int iter_tiles_x_of(int w) { return (w + 30) / 31; }
 inline int iter_tiles_of(int w, int h, int rows) { return iter_tiles_x_of(w) * ((h + rows - 1) / rows); }

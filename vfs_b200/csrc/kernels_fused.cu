@@ -9,14 +9,6 @@
 
 namespace vfs {
 
-// Locate the pair and the 32 x 8 tile of this block from the batch's tile ranges.
-template <class PairT, int N>
-__device__ __forceinline__ int find_pair(const PairT (&pr)[N], int npairs, int t) {
-  int k = 0;
-  while (k + 1 < npairs && t >= pr[k + 1].tile0) k++;
-  return k;
-}
-
 #define TILE_SETUP(ARGS)                                        \
   const int t_ = blockIdx.x;                                    \
   const int pi_ = find_pair(ARGS.pr, ARGS.npairs, t_);          \
@@ -46,9 +38,12 @@ struct FusedIter {
   // dual update at an in-image pixel whose code and tensor are given; returns false where
   // the pixel keeps its values (masked out), in which case tp is the stored (stale) T p.
   // u_pos and vp (u-bar and v-bar here) are returned for the threshold and primal steps.
+  // With want_th, also loads u, Iu and Iz of the pixel (read by the threshold step after the
+  // barrier) together with the dual step's loads, so they travel in the same round trip.
   static __device__ __forceinline__ bool dual_at(const IterPair& P, const T2* pin, const T4* qin, int ix, int iy,
                                                  int pos, uint8_t code, float a, float b, float c, float sp, float sq,
-                                                 float& u_pos, float2& vp, float2& p, float4& q, float2& tp) {
+                                                 float& u_pos, float2& vp, float2& p, float4& q, float2& tp,
+                                                 bool want_th, float& u_th, float& Iu_th, float& Iz_th) {
     int right = pos + 1, down = pos + P.s, left = pos - 1, up = pos - P.s;
     bool useRight, useDown;
     if (MASKED) {
@@ -77,6 +72,11 @@ struct FusedIter {
     float2 v_yn = useDown ? S::ld2(v_, down) : (up < 0 ? make_float2(0.f, 0.f) : S::ld2(v_, up));
     p = S::ld2(pin, pos);
     q = S::ld4(qin, pos);
+    if (want_th) {
+      u_th = P.u[pos];
+      Iu_th = P.Iu[pos];
+      Iz_th = P.Iz[pos];
+    }
     if (kFast) {
       fast::dual(useRight, useDown, u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
       tp = fast::tp(a, b, c, p);
@@ -121,18 +121,22 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   const bool tile = rx >= 1 && ry >= 1;
   const bool in_img = ix >= 0 && iy >= 0 && ix < P.w && iy < P.h;
   const int pos = ix + iy * P.s;
+  griddep_wait();  // the previous iteration's outputs are this one's inputs
+  griddep_launch_dependents();
 
   // ---- phase 1: dual update at every region pixel ------------------------------------
   float2 pp = make_float2(0.f, 0.f), tp = make_float2(0.f, 0.f), vb = make_float2(0.f, 0.f);
   float4 qq = make_float4(0.f, 0.f, 0.f, 0.f);
   uint8_t code = 0;
   float a = 0.f, b = 0.f, c = 0.f, ubar = 0.f;
+  float u_th = 0.f, Iu_th = 0.f, Iz_th = 0.f;
   if (in_img) {
     code = P.code[pos];
     a = P.a[pos];
     b = P.b[pos];
     c = P.c[pos];
-    bool own = F::dual_at(P, pin, qin, ix, iy, pos, code, a, b, c, A.sp[pi_], A.sq[pi_], ubar, vb, pp, qq, tp);
+    bool own = F::dual_at(P, pin, qin, ix, iy, pos, code, a, b, c, A.sp[pi_], A.sq[pi_], ubar, vb, pp, qq, tp, tile,
+                          u_th, Iu_th, Iz_th);
     if (own && tile) {
       S::st2(pout, pos, pp);
       S::st4(qout, pos, qq);
@@ -187,10 +191,10 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   float unew;
   if (kFast) {
     float eu = fast::etau(a, b, c, P.alpha1 * P.alpha1);
-    unew = fast::threshold(dxm, dym, eu, A.tau, ubar, P.u[pos], P.Iu[pos], P.Iz[pos], P.lambda);
+    unew = fast::threshold(dxm, dym, eu, A.tau, ubar, u_th, Iu_th, Iz_th, P.lambda);
   } else {
     float eu = etau_math(a, b, c, P.alpha1);
-    unew = threshold_math(dxm, dym, eu, A.tau, ubar, P.u[pos], P.Iu[pos], P.Iz[pos], P.lambda);
+    unew = threshold_math(dxm, dym, eu, A.tau, ubar, u_th, Iu_th, Iz_th, P.lambda);
   }
   P.us[pos] = unew;
 
@@ -217,13 +221,13 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
 
 template <int TH, int MINB, bool SINGLE>
 static void launch_iter_th2(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity) {
-  dim3 blk(32, TH + 1);
+  dim3 blk(32, TH + 1), grid(A.ntiles);
   if (masked) {
-    if (half_storage) k_fused_iter<true, __half, TH, MINB, SINGLE><<<A.ntiles, blk, 0, st>>>(A, parity);
-    else k_fused_iter<true, float, TH, MINB, SINGLE><<<A.ntiles, blk, 0, st>>>(A, parity);
+    if (half_storage) launch_overlapped(k_fused_iter<true, __half, TH, MINB, SINGLE>, grid, blk, st, A, parity);
+    else launch_overlapped(k_fused_iter<true, float, TH, MINB, SINGLE>, grid, blk, st, A, parity);
   } else {
-    if (half_storage) k_fused_iter<false, __half, TH, MINB, SINGLE><<<A.ntiles, blk, 0, st>>>(A, parity);
-    else k_fused_iter<false, float, TH, MINB, SINGLE><<<A.ntiles, blk, 0, st>>>(A, parity);
+    if (half_storage) launch_overlapped(k_fused_iter<false, __half, TH, MINB, SINGLE>, grid, blk, st, A, parity);
+    else launch_overlapped(k_fused_iter<false, float, TH, MINB, SINGLE>, grid, blk, st, A, parity);
   }
 }
 
@@ -237,6 +241,10 @@ void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, c
                             int variant) {
   if (A.ntiles <= 0) return;
   static_assert(kIterVariantRows[0] == 4 && kIterVariantRows[1] == 8 && kIterVariantRows[2] == 16, "variants");
+  if (variant >= kIterFirstRowsVariant && variant < kIterVariants) {
+    launch_fused_iteration_rows(A, masked, half_storage, st, parity, kIterVariantRows[variant]);
+    return;
+  }
   switch (variant) {
     case 0: launch_iter_th<4, kIterVariantMinBlocks[0]>(A, masked, half_storage, st, parity); break;
     case 2: launch_iter_th<16, kIterVariantMinBlocks[2]>(A, masked, half_storage, st, parity); break;

@@ -25,6 +25,11 @@ std::atomic<long long>& launch_counter() {
   return n;
 }
 
+std::atomic<bool>& pdl_enabled() {
+  static std::atomic<bool> on{true};
+  return on;
+}
+
 cudaEvent_t StereoTgvImpl::profEvent() {
   if (capture_events) {
     cudaEvent_t e;

@@ -44,6 +44,7 @@ class FusedEngine {
  public:
   bool use_graph = true;
   bool autotune = true;  // pick the iteration kernel's tile variant per level on first use
+  int forced_variant = -1;  // >= 0: this iteration-kernel variant at every level (no tuning)
   // tuned tile variant per level, keyed by batch composition (form, storage, sizes)
   const std::map<std::vector<int>, std::vector<int>>& tuned() const { return tuned_; }
   ~FusedEngine();

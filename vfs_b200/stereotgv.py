@@ -92,6 +92,10 @@ class StereoTgv:
     def set_autotune(self, on: bool) -> None:
         check(self._h, self._L.vfs_set_autotune(self._h, int(on)))
 
+    def set_iteration_variant(self, variant: int) -> None:
+        """Force one variant (0..5) of the fused iteration kernel, or -1 for the tuned choice."""
+        check(self._h, self._L.vfs_set_iteration_variant(self._h, int(variant)))
+
     # ---- reference methods -------------------------------------------------
     def initialize(self, width, height, beta, gamma, alpha0, alpha1, timestep_lambda, lambda_,
                    nLevels, fScale, nWarpIters, nSolverIters) -> int:
@@ -285,6 +289,10 @@ class StereoBatch:
 
     def set_autotune(self, on: bool) -> None:
         check_batch(self._h, self._L.vfs_batch_set_autotune(self._h, int(on)))
+
+    def set_iteration_variant(self, variant: int) -> None:
+        """Force one variant (0..5) of the fused iteration kernel, or -1 for the tuned choice."""
+        check_batch(self._h, self._L.vfs_batch_set_iteration_variant(self._h, int(variant)))
 
     def set_mode(self, one_launch: bool) -> None:
         """False (default): pairs run concurrently, each from its own CUDA graph; True: one
