@@ -105,12 +105,19 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   constexpr bool kFast = F::kFast;
   __shared__ float2 sTp[TH + 1][32];
   __shared__ float4 sQ[TH + 1][32];
+  // one pair: a 2-D grid of tiles; several pairs: a 1-D grid over the pairs' tile ranges
   const int t_ = blockIdx.x;
   const int pi_ = SINGLE ? 0 : find_pair(A.pr, A.npairs, t_);
   const IterPair& P = A.pr[pi_];
-  const int lt_ = t_ - P.tile0;
-  const int x0 = (lt_ % P.tiles_x) * 31;
-  const int y0 = (lt_ / P.tiles_x) * TH;
+  int x0, y0;
+  if (SINGLE) {
+    x0 = (int)blockIdx.x * 31;
+    y0 = (int)blockIdx.y * TH;
+  } else {
+    const int lt_ = t_ - P.tile0;
+    x0 = (lt_ % P.tiles_x) * 31;
+    y0 = (lt_ / P.tiles_x) * TH;
+  }
   const int rx = threadIdx.x, ry = threadIdx.y;
   const int ix = x0 - 1 + rx, iy = y0 - 1 + ry;
   const int plane = P.s * P.h;
@@ -135,6 +142,11 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
     a = P.a[pos];
     b = P.b[pos];
     c = P.c[pos];
+  }
+  // masked form: a block with no pixel on in its region writes nothing and reads nothing
+  // another block needs, so it leaves here
+  if (MASKED && !__syncthreads_or(in_img && (code & kOn))) return;
+  if (in_img) {
     bool own = F::dual_at(P, pin, qin, ix, iy, pos, code, a, b, c, A.sp[pi_], A.sq[pi_], ubar, vb, pp, qq, tp, tile,
                           u_th, Iu_th, Iz_th);
     if (own && tile) {
@@ -222,6 +234,7 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
 template <int TH, int MINB, bool SINGLE>
 static void launch_iter_th2(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity) {
   dim3 blk(32, TH + 1), grid(A.ntiles);
+  if (SINGLE) grid = dim3(A.pr[0].tiles_x, (A.pr[0].h + TH - 1) / TH);
   if (masked) {
     if (half_storage) launch_overlapped(k_fused_iter<true, __half, TH, MINB, SINGLE>, grid, blk, st, A, parity);
     else launch_overlapped(k_fused_iter<true, float, TH, MINB, SINGLE>, grid, blk, st, A, parity);
