@@ -372,9 +372,16 @@ def run_ours(args, rank, world, local):
     iv = np.concatenate([s.profile_intervals(kind) for s in solvers])
     for s in solvers:
         s.profile(False)
-    n_l, pi_l = len(iv), float(iv[:, 2].sum()) if len(iv) else 0.0
-    ms_l = union_ms(iv[:, :2]) if len(iv) else 0.0
-    ms_sum = float((iv[:, 1] - iv[:, 0]).sum()) if len(iv) else 0.0
+    # all levels, and the dominant kernel alone: the iteration kernel at full resolution (the
+    # records with the largest pixel count)
+    pi_all = float(iv[:, 2].sum()) if len(iv) else 0.0
+    ms_all = union_ms(iv[:, :2]) if len(iv) else 0.0
+    top = iv[iv[:, 2] == iv[:, 2].max()] if len(iv) else iv
+    pi_l = float(top[:, 2].sum()) if len(top) else 0.0
+    n_launch = int(top[:, 3].sum()) if len(top) else 0
+    ms_l = union_ms(top[:, :2]) if len(top) else 0.0
+    ms_sum = float((top[:, 1] - top[:, 0]).sum()) if len(top) else 0.0
+    variants = solvers[0].iteration_variants() if fused else []
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
@@ -434,13 +441,9 @@ def run_ours(args, rank, world, local):
         peak, peak_kind = measured_peak()
         b_alg = B_ALG_FP16 if half else B_ALG_FP32
         achieved = (pi_l * b_alg / (ms_l / 1000.0) / 1e9) if ms_l > 0 else None
+        achieved_all = (pi_all * b_alg / (ms_all / 1000.0) / 1e9) if ms_all > 0 else None
         storage = "fp16" if half else "fp32"
         kernel_key = f"fused_inner_{storage}" if args.path == "fused" else "plain_inner_iteration"
-        # one fused record covers nSolverIters launches of k_fused_iter; one drop-in record
-        # covers one iteration (its four kernels)
-        from vfs_b200 import synth
-        per_rec = synth.SOLVER_PARAMS["nSolverIters"] if fused else 1
-        n_launch = n_l * per_rec
         px_per_launch = pi_l / n_launch if n_launch else 0.0
         tr = ncu_traffic(kernel_key)
         traffic = None
@@ -459,13 +462,17 @@ def run_ours(args, rank, world, local):
                            "note": "per frame; a batched step completes all its frames together"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                         "kernel": "k_fused_iter" if fused else "drop-in inner iteration",
+                         "kernel": ("full-resolution fused iteration (variant %s)" % (variants[0] if variants else "?"))
+                         if fused else "drop-in inner iteration at full resolution",
                          "launches_measured": int(n_launch),
                          "algorithmic_bytes_per_launch": b_alg * px_per_launch,
                          "bytes_per_pixel_iteration": b_alg, "peak_kind": peak_kind,
-                         "time_basis": "union of the inner-loop event intervals of all pairs in the last timed "
-                                       "step (concurrent pairs overlap)",
+                         "time_basis": "union of the full-resolution inner-loop event intervals of all pairs "
+                                       "in the last timed step (concurrent pairs overlap)",
                          "busy_ms": ms_l, "sum_of_interval_ms": ms_sum,
+                         "all_levels": {"achieved": achieved_all, "frac": (achieved_all / peak) if achieved_all else None,
+                                        "busy_ms": ms_all},
+                         "iteration_variants_by_level": variants,
                          "traffic_source": "profiles/roofline_traffic.json (ncu) x pixels per launch"
                          if traffic is not None else None},
             "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": batch * 2 * W0 * H0,

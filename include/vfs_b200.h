@@ -165,10 +165,16 @@ int vfs_set_autotune(vfs_stereo* s, int on);
 /* Force one variant of the fused iteration kernel at every pyramid level (-1: the tuned or
  * default choice).  0-2: 32 x (4, 8, 16 + 1)-thread blocks exchanging the west / north
  * neighbours' T p and q through shared memory; 3-5: one warp per 31-column strip of 8, 16
- * or 32 rows, neighbours by warp shuffle and registers.  Every variant gives the same
- * results; this selects speed only.  (No counterpart in the reference.) */
-#define VFS_ITER_VARIANTS 6
+ * or 32 rows, neighbours by warp shuffle and registers; 6-9: several iterations per launch
+ * with the tile's region held in shared memory (6: 3 iterations on 64 x 24 tiles, 7: 5 on
+ * 32 x 24, 8: 3 on 23 x 23, 9: 5 on 17 x 17), for one-pair launches (other launches, and
+ * levels where it does not apply, use variant 1).  Every variant gives the same results;
+ * this selects speed only.  (No counterpart in the reference.) */
+#define VFS_ITER_VARIANTS 10
 int vfs_set_iteration_variant(vfs_stereo* s, int variant);
+/* The variant each pyramid level (finest first) used in the handle's last fused solve
+ * (tuned, default or forced); *count receives the number of levels. */
+int vfs_get_iteration_variants(vfs_stereo* s, int* variants, int max_levels, int* count);
 int vfs_batch_set_iteration_variant(vfs_batch* b, int variant);
 
 /* Histogram equalisation of n 8-bit pixels in device memory (d_dst may equal d_src), as
@@ -212,14 +218,14 @@ int vfs_profile_read(vfs_stereo* s, int kind, long long* launches, double* total
                      double* pixel_iterations);
 /* vfs_profile_epoch() records one process-wide reference event on a stream (NULL: the
  * legacy default stream).  vfs_profile_intervals() then returns, for the handle's records
- * of a kind, their start and end in ms after that event and their pixel-iterations (up
- * to max_records of them; *count receives the number of records).  Records of handles
+ * of a kind, their start and end in ms after that event, their pixel-iterations and their
+ * kernel launches (up to max_records of them; *count receives the number of records).  Records of handles
  * solved concurrently on different streams overlap; their union is the time during which
  * at least one such group ran.  A graph replay re-records the events captured with it, so
  * after several replays the records describe the last one. */
 int vfs_profile_epoch(void* cuda_stream);
 int vfs_profile_intervals(vfs_stereo* s, int kind, int max_records, double* start_ms, double* end_ms,
-                          double* pixel_iterations, int* count);
+                          double* pixel_iterations, double* launches, int* count);
 
 /* ---- reference DLL entry points (dllhook/vfs.h:37-44) -------------------------------
  * Create / Init / SolveStereo with the reference's names and argument lists.  Init reads

@@ -78,6 +78,7 @@ SIGNATURES = {
     "vfs_batch_set_mode": [_vp, _i],
     "vfs_set_autotune": [_vp, _i],
     "vfs_set_iteration_variant": [_vp, _i],
+    "vfs_get_iteration_variants": [_vp, _vp, _i, ctypes.POINTER(_i)],
     "vfs_batch_set_iteration_variant": [_vp, _i],
     "vfs_equalize_hist_u8": [_vp, _vp, _sz, _vp],
     "vfs_equalize_hist_u8_noalloc": [_vp, _vp, _sz, _i, _vp],
@@ -89,7 +90,7 @@ SIGNATURES = {
     "vfs_profile_read": [_vp, _i, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),
                          ctypes.POINTER(ctypes.c_double)],
     "vfs_profile_epoch": [_vp],
-    "vfs_profile_intervals": [_vp, _i, _i, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int)],
+    "vfs_profile_intervals": [_vp, _i, _i, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int)],
     "Create": [],
     "Init": [_vp, _i, _i, _f, _f, _f, _f, _f, _f, _i, _f, _i, _i, _f, _f, ctypes.c_char_p, ctypes.c_char_p,
              ctypes.c_char_p],

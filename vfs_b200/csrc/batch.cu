@@ -34,8 +34,12 @@ void set_iter_tiles(IterArgs& A, int k, int w, int h, int rows) {
 // level_variant[l]: tile variant of the iteration kernel at level l; -1 = time the
 // variants on this level's data before its first iteration (only when can_tune) and
 // store the fastest there.
+// concurrency: one-pair solves running at the same time on other streams (the batch's
+// concurrent mode); the tuner's cost of a variant is its time per iteration times the larger
+// of the share of the GPU its launches occupy and 1 / concurrency, so that with several pairs
+// in flight it weighs the GPU time a variant takes from the others, and alone its latency.
 void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st,
-                        std::vector<int>& level_variant, bool can_tune) {
+                        std::vector<int>& level_variant, bool can_tune, int concurrency) {
   const int n = (int)pairs.size();
   if (n == 0) return;
   if (n > kMaxPairs) throw ArgError{"batch larger than " + std::to_string(kMaxPairs) + " pairs"};
@@ -197,29 +201,64 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         A.npairs = na;
         return A;
       };
+      // the K-iterations-per-launch kernel: one pair per launch, and exact at this level
+      const bool tb_here = na == 1 && (!masked || (level < (int)act[0]->tb_ok.size() && act[0]->tb_ok[level]));
+      auto tb_args = [&](float sigma_, float tau_, int iter0, int k) {
+        IterTBArgs T{};
+        T.P = iter_args(kIterDefaultVariant, sigma_, tau_, 1.0f, 0).pr[0];
+        for (int j = 0; j < k; j++) {
+          float mu_;
+          if (sigma_ < 1000.0f) mu_ = 1.0f / std::sqrt(1 + 0.7f * tau_ * P0.timestep_lambda);
+          else mu_ = 1;
+          T.sp[j] = act[0]->P.alpha1 * sigma_ / 3.0f;
+          T.sq[j] = act[0]->P.alpha0 * sigma_ / 2.0f;
+          T.tau[j] = tau_;
+          T.mu[j] = mu_;
+          sigma_ = sigma_ / mu_;
+          tau_ = tau_ * mu_;
+        }
+        T.parity = iter0 & 1;
+        T.write_tp = 0;
+        return T;
+      };
       if (level_variant[level] < 0) {
         if (can_tune && warpIter == 0 && P0.nSolverIters > 0) {
           // Time every tile variant on this level's data.  These launches read the same
           // inputs as the first iteration below and write only what it overwrites (the
           // other p / q plane, us, u_s, v_s at in-mask pixels; T p is left alone), so they
           // do not change any result.
-          float best = 1e30f;
+          double best = 1e30;
           int best_v = kIterDefaultVariant;
+          const double floor_share = 1.0 / (double)std::max(1, concurrency);
           float mu0 = 1.0f / std::sqrt(1 + 0.7f * 1.0f * P0.timestep_lambda);
           cudaEvent_t e0, e1;
           VFS_CUDA(cudaEventCreate(&e0));
           VFS_CUDA(cudaEventCreate(&e1));
           for (int v = 0; v < kIterVariants; v++) {
-            IterArgs T = iter_args(v, 1.0f, 1.0f, mu0, 0);
-            launch_fused_iteration(T, masked, half, st, 0, v);  // warm the caches / the instruction path
+            // the row-streaming forms are slower everywhere on B200 (one warp walks its strip
+            // serially); they stay available as forced variants
+            if (v >= kIterFirstRowsVariant && v < kIterFirstTBVariant) continue;
+            const int kv = tb_iterations(v);
+            if (kv > 1 && (!tb_here || kv > P0.nSolverIters)) continue;
+            IterArgs T = iter_args(kv > 1 ? kIterDefaultVariant : v, 1.0f, 1.0f, mu0, 0);
+            IterTBArgs TB = tb_args(1.0f, 1.0f, 0, kv);
+            auto once = [&] {
+              if (kv > 1) launch_fused_iteration_tb(TB, masked, half, st, v);
+              else launch_fused_iteration(T, masked, half, st, 0, v);
+            };
+            once();  // warm the caches / the instruction path
             VFS_CUDA(cudaEventRecord(e0, st));
-            for (int r = 0; r < 3; r++) launch_fused_iteration(T, masked, half, st, 0, v);
+            for (int r = 0; r < 3; r++) once();
             VFS_CUDA(cudaEventRecord(e1, st));
             VFS_CUDA(cudaEventSynchronize(e1));
             float ms = 0;
             VFS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            if (ms < best) {
-              best = ms;
+            ms /= (float)kv;  // per iteration
+            double share = 1.0;
+            if (na == 1) share = iteration_gpu_share(v, masked, half, act[0]->pW[level], act[0]->pH[level]);
+            const double cost = (double)ms * std::max(share, floor_share);
+            if (cost < best) {
+              best = cost;
               best_v = v;
             }
           }
@@ -231,24 +270,43 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         }
       }
       const int variant = level_variant[level] < 0 ? kIterDefaultVariant : level_variant[level];
+      // K iterations per launch where the variant is a multi-iteration one and it applies
+      // here; the remaining iterations (and the fallback) use the default one-iteration form
+      const int K = tb_here ? tb_iterations(variant) : 1;
+      const int v1 = tb_iterations(variant) > 1 ? kIterDefaultVariant : variant;
       float tau = 1.0f;
       float sigma = 1.0f / tau;
-      prof->profBeginPx(kProfFused, px_level, P0.nSolverIters, st);
-      for (int iter = 0; iter < P0.nSolverIters; iter++) {
-        float mu;
-        if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P0.timestep_lambda);
-        else mu = 1;
-        IterArgs A = iter_args(variant, sigma, tau, mu, iter == P0.nSolverIters - 1);
-        launch_fused_iteration(A, masked, half, st, iter & 1, variant);
-        for (auto* s : act) {
-          std::swap(s->d_u, s->d_us);
-          std::swap(s->d_u_, s->d_u_s);
-          if (half) std::swap(s->f_vh, s->f_vhs);
-          else std::swap(s->d_v_, s->d_v_s);
-          s->f_parity = (iter & 1) ? 0 : 1;
+      const int n_it = P0.nSolverIters;
+      prof->profBeginPx(kProfFused, px_level, n_it, st, K > 1 ? n_it / K + n_it % K : n_it);
+      for (int iter = 0; iter < n_it;) {
+        const int k = (K > 1 && iter + K <= n_it) ? K : 1;
+        if (k > 1) {
+          IterTBArgs T = tb_args(sigma, tau, iter, k);
+          T.write_tp = iter + k == n_it;
+          launch_fused_iteration_tb(T, masked, half, st, variant);
+          for (int j = 0; j < k; j++) {
+            sigma = sigma / T.mu[j];
+            tau = tau * T.mu[j];
+          }
+        } else {
+          float mu;
+          if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P0.timestep_lambda);
+          else mu = 1;
+          IterArgs A = iter_args(v1, sigma, tau, mu, iter == n_it - 1);
+          launch_fused_iteration(A, masked, half, st, iter & 1, v1);
+          sigma = sigma / mu;
+          tau = tau * mu;
         }
-        sigma = sigma / mu;
-        tau = tau * mu;
+        for (int it = iter; it < iter + k; it++) {
+          for (auto* s : act) {
+            std::swap(s->d_u, s->d_us);
+            std::swap(s->d_u_, s->d_u_s);
+            if (half) std::swap(s->f_vh, s->f_vhs);
+            else std::swap(s->d_v_, s->d_v_s);
+            s->f_parity = (it & 1) ? 0 : 1;
+          }
+        }
+        iter += k;
       }
       prof->profEnd(st);
       prof->profBeginPx(kProfEpilogue, px_level, 1, st);
@@ -348,6 +406,19 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
     if (masked && !s->codes_valid) {
       for (int l = 0; l < s->levels(); l++)
         launch_edge_codes(s->pMask[l], s->code_masked[l], s->pW[l], s->pH[l], s->pS[l], s->stream());
+      // a level without row padding reads the previous row's last pixel west of column 0;
+      // the multi-iteration kernel cannot follow that pixel, so it is used there only when
+      // no pixel of column 0 is on
+      s->tb_ok.assign(s->levels(), 1);
+      for (int l = 0; l < s->levels(); l++) {
+        if (s->pW[l] != s->pS[l]) continue;
+        std::vector<uint8_t> col(s->pH[l]);
+        VFS_CUDA(cudaMemcpy2DAsync(col.data(), 1, s->code_masked[l], s->pS[l], 1, s->pH[l], cudaMemcpyDeviceToHost,
+                                   s->stream()));
+        VFS_CUDA(cudaStreamSynchronize(s->stream()));
+        for (uint8_t c : col)
+          if (c & kOn) s->tb_ok[l] = 0;
+      }
       s->codes_valid = true;
     }
   }
@@ -365,7 +436,7 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     maxL = std::max(maxL, s->levels());
   }
   std::sort(geo.begin(), geo.end());
-  std::vector<int> comp{(int)masked, (int)half};
+  std::vector<int> comp{(int)masked, (int)half, concurrency};
   for (auto& g : geo) comp.insert(comp.end(), g.begin(), g.end());
   auto tit = tuned_.find(comp);
   if (tit == tuned_.end() && forced_variant >= 0) tit = tuned_.emplace(comp, std::vector<int>(maxL, forced_variant)).first;
@@ -373,16 +444,18 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     std::vector<int> lv(maxL, autotune ? -1 : kIterDefaultVariant);
     if (autotune) {
       // first solve of this composition: run it directly and tune while it runs
-      fused_solve_direct(pairs, masked, half, st, lv, true);
+      fused_solve_direct(pairs, masked, half, st, lv, true, concurrency);
       tuned_[comp] = lv;
+      last_variants = lv;
       return;
     }
     tit = tuned_.emplace(comp, lv).first;
   }
   std::vector<int> variants = tit->second;
   if (forced_variant >= 0) variants.assign(maxL, forced_variant);
+  last_variants = variants;
   if (!use_graph) {
-    fused_solve_direct(pairs, masked, half, st, variants, false);
+    fused_solve_direct(pairs, masked, half, st, variants, false, concurrency);
     return;
   }
   StereoTgvImpl* prof = pairs[0];
@@ -410,7 +483,7 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     long long launches0 = launch_counter().load();
     VFS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
     try {
-      fused_solve_direct(pairs, masked, half, st, variants, false);
+      fused_solve_direct(pairs, masked, half, st, variants, false, concurrency);
     } catch (...) {
       prof->capture_events = nullptr;
       cudaGraph_t junk = nullptr;

@@ -349,6 +349,14 @@ int vfs_set_iteration_variant(vfs_stereo* s, int variant) {
   });
 }
 
+int vfs_get_iteration_variants(vfs_stereo* s, int* variants, int max_levels, int* count) {
+  return guarded(s, [&] {
+    const std::vector<int>& v = s->impl.engine.last_variants;
+    if (count) *count = (int)v.size();
+    for (int l = 0; l < max_levels && l < (int)v.size(); l++) variants[l] = v[l];
+  });
+}
+
 int vfs_batch_set_iteration_variant(vfs_batch* b, int variant) {
   return guarded(b, [&] {
     if (variant < -1 || variant >= vfs::kIterVariants) throw vfs::ArgError{"iteration variant out of range"};
@@ -418,21 +426,24 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
       std::vector<vfs::StereoTgvImpl*> one{pairs[k]};
       vfs::FusedEngine& eng = pairs[k]->engine;
       const bool g = eng.use_graph, t = eng.autotune;
-      const int fv = eng.forced_variant;
+      const int fv = eng.forced_variant, cc = eng.concurrency;
       eng.use_graph = b->engine.use_graph;
       eng.autotune = b->engine.autotune;
       eng.forced_variant = b->engine.forced_variant;
-      try {
-        eng.solve(one, masked != 0, b->half, b->lanes[k]);
-      } catch (...) {
+      eng.concurrency = (int)pairs.size();
+      auto restore = [&] {
         eng.use_graph = g;
         eng.autotune = t;
         eng.forced_variant = fv;
+        eng.concurrency = cc;
+      };
+      try {
+        eng.solve(one, masked != 0, b->half, b->lanes[k]);
+      } catch (...) {
+        restore();
         throw;
       }
-      eng.use_graph = g;
-      eng.autotune = t;
-      eng.forced_variant = fv;
+      restore();
       if (io) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, b->lanes[k]);
       VFS_CUDA(cudaEventRecord(b->lane_done[k], b->lanes[k]));
       VFS_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
@@ -528,7 +539,7 @@ int vfs_profile_epoch(void* cuda_stream) {
 }
 
 int vfs_profile_intervals(vfs_stereo* s, int kind, int max_records, double* start_ms, double* end_ms,
-                          double* pixel_iterations, int* count) {
+                          double* pixel_iterations, double* launches, int* count) {
   return guarded(s, [&] {
     if (kind < 0 || kind >= vfs::kProfTags) throw vfs::ArgError{"profile kind out of range"};
     if (!g_prof_epoch) throw vfs::ArgError{"vfs_profile_epoch() has not been recorded"};
@@ -545,6 +556,7 @@ int vfs_profile_intervals(vfs_stereo* s, int kind, int max_records, double* star
         if (start_ms) start_ms[n] = a;
         if (end_ms) end_ms[n] = b;
         if (pixel_iterations) pixel_iterations[n] = (double)r.px * r.iters;
+        if (launches) launches[n] = (double)r.launches;
       }
       n++;
     }

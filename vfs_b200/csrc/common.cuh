@@ -41,6 +41,7 @@ struct ProfRec {
   long long px;   // pixels of the level
   int iters;      // inner iterations covered by the record
   cudaEvent_t a, b;
+  int launches;   // kernel launches of the record's group
 };
 enum ProfTag { kProfInner = 0, kProfFused = 1, kProfPrologue = 2, kProfEpilogue = 3, kProfTags = 4 };
 
@@ -59,15 +60,16 @@ __device__ __forceinline__ void griddep_launch_dependents() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 template <typename... KArgs, typename... Args>
-inline void launch_overlapped(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+inline void launch_overlapped_smem(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                                   Args... args) {
   if (!pdl_enabled().load(std::memory_order_relaxed)) {
-    k<<<grid, block, 0, st>>>(args...);
+    k<<<grid, block, smem, st>>>(args...);
     return;
   }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute at[1];
   at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -75,6 +77,10 @@ inline void launch_overlapped(void (*k)(KArgs...), dim3 grid, dim3 block, cudaSt
   cfg.attrs = at;
   cfg.numAttrs = 1;
   VFS_CUDA(cudaLaunchKernelEx(&cfg, k, args...));
+}
+template <typename... KArgs, typename... Args>
+inline void launch_overlapped(void (*k)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+  launch_overlapped_smem(k, grid, block, 0, st, args...);
 }
 
 inline int iDivUp(int n, int m) { return (n + m - 1) / m; }

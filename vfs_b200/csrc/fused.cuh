@@ -36,6 +36,13 @@ struct Store2<float> {
   static __device__ __forceinline__ void st2(T2* b, long long k, float2 v) { b[k] = v; }
   static __device__ __forceinline__ float4 ld4(const T4* b, long long k) { return b[k]; }
   static __device__ __forceinline__ void st4(T4* b, long long k, float4 v) { b[k] = v; }
+  // conversions between the stored form and float (identities here)
+  static __device__ __forceinline__ T2 ld2z() { return make_float2(0.f, 0.f); }
+  static __device__ __forceinline__ T4 ld4z() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+  static __device__ __forceinline__ float2 cvt2(T2 v) { return v; }
+  static __device__ __forceinline__ float4 cvt4(T4 v) { return v; }
+  static __device__ __forceinline__ T2 rnd2(float2 v) { return v; }
+  static __device__ __forceinline__ T4 rnd4(float4 v) { return v; }
 };
 template <>
 struct Store2<__half> {
@@ -48,11 +55,26 @@ struct Store2<__half> {
     float2 x = __half22float2(t.a), y = __half22float2(t.b);
     return make_float4(x.x, x.y, y.x, y.y);
   }
-  static __device__ __forceinline__ void st4(T4* b, long long k, float4 v) {
+  static __device__ __forceinline__ void st4(T4* b, long long k, float4 v) { b[k] = rnd4(v); }
+  // conversions between the stored form and float, the same roundings as ld / st above
+  static __device__ __forceinline__ T2 ld2z() { return __floats2half2_rn(0.f, 0.f); }
+  static __device__ __forceinline__ T4 ld4z() {
+    T4 t;
+    t.a = ld2z();
+    t.b = ld2z();
+    return t;
+  }
+  static __device__ __forceinline__ float2 cvt2(T2 v) { return __half22float2(v); }
+  static __device__ __forceinline__ float4 cvt4(T4 t) {
+    float2 x = __half22float2(t.a), y = __half22float2(t.b);
+    return make_float4(x.x, x.y, y.x, y.y);
+  }
+  static __device__ __forceinline__ T2 rnd2(float2 v) { return __float22half2_rn(v); }
+  static __device__ __forceinline__ T4 rnd4(float4 v) {
     T4 t;
     t.a = __float22half2_rn(make_float2(v.x, v.y));
     t.b = __float22half2_rn(make_float2(v.z, v.w));
-    b[k] = t;
+    return t;
   }
 };
 
@@ -94,6 +116,23 @@ void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, c
 // the row-streaming form with `rows` (8, 16 or 32) output rows per warp
 void launch_fused_iteration_rows(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
                                  int rows);
+
+// ---- K consecutive primal-dual iterations of one pair in one launch (kernels_tb.cu) ----
+constexpr int kIterTBMax = 5;
+struct IterTBArgs {
+  IterPair P;  // pointers of the launch's first iteration (its outputs: us, u_s, v_s)
+  float sp[kIterTBMax], sq[kIterTBMax], tau[kIterTBMax], mu[kIterTBMax];  // per iteration
+  int parity;    // p / q plane read by the first iteration
+  int write_tp;  // 1: the last iteration of the launch stores T p
+};
+// iterations per launch of an iteration-kernel variant (1 for the one-iteration forms)
+int tb_iterations(int variant);
+// Fraction of the GPU's resident-block capacity that one launch of a variant for one pair of
+// w x h pixels occupies (1 when it fills or exceeds a wave); the tuner's cost model.
+double iteration_gpu_share(int variant, bool masked, bool half, int w, int h);
+double rows_gpu_share(int variant, bool masked, bool half, int w, int h);
+double tb_gpu_share(int variant, bool masked, bool half, int w, int h);
+void launch_fused_iteration_tb(const IterTBArgs& A, bool masked, bool half_storage, cudaStream_t st, int variant);
 
 // ---- per-warp prologue: zero p, q, v-bar; resample tv at x + warpUV; warp I1 ----
 struct WarpStartPair {
@@ -202,10 +241,14 @@ inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFT
 // Variants 0-2: k_fused_iter (32 x (rows + 1) blocks, shared-memory west / north exchange);
 // variants 3-5: k_fused_iter_rows (one warp walks down a 31-column strip of `rows` rows,
 // neighbours by shuffle and registers; kernels_rows.cu).  All give identical results.
-constexpr int kIterVariants = 6;
-constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32};
-constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0};
+// variants 6-9: k_fused_iter_tb, several iterations per launch with the tile's region in
+// shared memory (kernels_tb.cu), one pair per launch only: 3 iterations on 64 x 24 tiles,
+// 5 on 32 x 24, and with one region pixel per thread 3 on 23 x 23 and 5 on 17 x 17 tiles.
+constexpr int kIterVariants = 10;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0};
 constexpr int kIterFirstRowsVariant = 3;
+constexpr int kIterFirstTBVariant = 6;
 constexpr int kIterDefaultVariant = 1;
 inline int iter_tiles_x_of(int w) { return (w + 30) / 31; }
 inline int iter_tiles_of(int w, int h, int rows) { return iter_tiles_x_of(w) * ((h + rows - 1) / rows); }

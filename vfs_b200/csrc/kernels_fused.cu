@@ -250,11 +250,51 @@ static void launch_iter_th(const IterArgs& A, bool masked, bool half_storage, cu
   else launch_iter_th2<TH, MINB, false>(A, masked, half_storage, st, parity);
 }
 
+namespace {
+template <int TH, int MINB>
+int blocks_per_sm_th(bool masked, bool half) {
+  int n = 0;
+  const int threads = 32 * (TH + 1);
+  if (masked) {
+    if (half) VFS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_iter<true, __half, TH, MINB, true>, threads, 0));
+    else VFS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_iter<true, float, TH, MINB, true>, threads, 0));
+  } else {
+    if (half) VFS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_iter<false, __half, TH, MINB, true>, threads, 0));
+    else VFS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_iter<false, float, TH, MINB, true>, threads, 0));
+  }
+  return n;
+}
+}  // namespace
+
+double iteration_gpu_share(int variant, bool masked, bool half, int w, int h) {
+  // blocks of the launch and resident blocks per SM of the variant's kernel (one pair)
+  long long blocks = 0;
+  int per_sm = 0;
+  if (variant >= kIterFirstTBVariant) {
+    return tb_gpu_share(variant, masked, half, w, h);
+  } else if (variant >= kIterFirstRowsVariant) {
+    return rows_gpu_share(variant, masked, half, w, h);
+  } else {
+    const int rows = kIterVariantRows[variant];
+    blocks = (long long)iter_tiles_of(w, h, rows);
+    switch (variant) {
+      case 0: per_sm = blocks_per_sm_th<4, kIterVariantMinBlocks[0]>(masked, half); break;
+      case 2: per_sm = blocks_per_sm_th<16, kIterVariantMinBlocks[2]>(masked, half); break;
+      default: per_sm = blocks_per_sm_th<8, kIterVariantMinBlocks[1]>(masked, half); break;
+    }
+  }
+  int dev = 0, sms = 1;
+  VFS_CUDA(cudaGetDevice(&dev));
+  VFS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const double cap = (double)sms * (per_sm > 0 ? per_sm : 1);
+  return blocks >= cap ? 1.0 : (double)blocks / cap;
+}
+
 void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
                             int variant) {
   if (A.ntiles <= 0) return;
   static_assert(kIterVariantRows[0] == 4 && kIterVariantRows[1] == 8 && kIterVariantRows[2] == 16, "variants");
-  if (variant >= kIterFirstRowsVariant && variant < kIterVariants) {
+  if (variant >= kIterFirstRowsVariant && variant < kIterFirstTBVariant) {
     launch_fused_iteration_rows(A, masked, half_storage, st, parity, kIterVariantRows[variant]);
     return;
   }

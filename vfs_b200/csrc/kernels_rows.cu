@@ -343,6 +343,34 @@ static void launch_rows(const IterArgs& A, bool masked, bool half_storage, cudaS
   else launch_rows2<R, false>(A, masked, half_storage, st, parity);
 }
 
+namespace {
+template <int R>
+int rows_blocks_per_sm(bool masked, bool half) {
+  int n = 0;
+  const int threads = 32 * kRowWarps;
+  if (masked) {
+    if (half) VFS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_iter_rows<true, __half, R, true>, threads, 0));
+    else VFS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_iter_rows<true, float, R, true>, threads, 0));
+  } else {
+    if (half) VFS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_iter_rows<false, __half, R, true>, threads, 0));
+    else VFS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fused_iter_rows<false, float, R, true>, threads, 0));
+  }
+  return n;
+}
+}  // namespace
+
+double rows_gpu_share(int variant, bool masked, bool half, int w, int h) {
+  const int R = kIterVariantRows[variant];
+  const long long blocks = ((long long)iter_tiles_of(w, h, R) + kRowWarps - 1) / kRowWarps;
+  int per_sm = R == 8 ? rows_blocks_per_sm<8>(masked, half) : R == 32 ? rows_blocks_per_sm<32>(masked, half)
+                                                                     : rows_blocks_per_sm<16>(masked, half);
+  int dev = 0, sms = 1;
+  VFS_CUDA(cudaGetDevice(&dev));
+  VFS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const double cap = (double)sms * (per_sm > 0 ? per_sm : 1);
+  return blocks >= cap ? 1.0 : (double)blocks / cap;
+}
+
 void launch_fused_iteration_rows(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
                                  int rows) {
   if (A.ntiles <= 0) return;

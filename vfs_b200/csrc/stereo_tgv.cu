@@ -54,9 +54,9 @@ void StereoTgvImpl::profBegin(int tag, int level, int iters) {
   profBeginPx(tag, (long long)pW[level] * pH[level], iters);
 }
 
-void StereoTgvImpl::profBeginPx(int tag, long long px, int iters, cudaStream_t st) {
+void StereoTgvImpl::profBeginPx(int tag, long long px, int iters, cudaStream_t st, int launches) {
   if (!profiling) return;
-  ProfRec r{tag, 0, px, iters, profEvent(), profEvent()};
+  ProfRec r{tag, 0, px, iters, profEvent(), profEvent(), launches > 0 ? launches : iters};
   record(r.a, st ? st : stream_, capture_events != nullptr);
   prof_.push_back(r);
 }

@@ -45,6 +45,7 @@ class FusedEngine {
   bool use_graph = true;
   bool autotune = true;  // pick the iteration kernel's tile variant per level on first use
   int forced_variant = -1;  // >= 0: this iteration-kernel variant at every level (no tuning)
+  int concurrency = 1;      // one-pair solves run at the same time (set by a concurrent batch)
   // tuned tile variant per level, keyed by batch composition (form, storage, sizes)
   const std::map<std::vector<int>, std::vector<int>>& tuned() const { return tuned_; }
   ~FusedEngine();
@@ -53,6 +54,8 @@ class FusedEngine {
   // allocate fused buffers and refresh edge codes, each on the pair's own stream
   static void prepare(std::vector<StereoTgvImpl*>& pairs, bool masked);
   size_t graphs() const { return cache_.size(); }
+  // iteration-kernel variant per pyramid level (finest first) of the last solve
+  std::vector<int> last_variants;
 
  private:
   struct Entry {
@@ -117,6 +120,9 @@ class StereoTgvImpl {
   void* f_vhs = nullptr; // other half v-bar
   std::vector<uint8_t*> code_masked, code_plain;
   bool codes_valid = false;
+  // per level: the K-iterations-per-launch kernel reproduces the masked form exactly (false
+  // only when the row has no padding and a pixel of column 0 is on; kernels_tb.cu)
+  std::vector<uint8_t> tb_ok;
   int f_parity = 0;      // which p / q plane holds the latest values
   int levels() const { return (int)pW.size(); }
   Geom geomAt(int level) const { return Geom{pW[level], pH[level], pS[level]}; }
@@ -173,7 +179,8 @@ class StereoTgvImpl {
   cudaEvent_t profEvent();
   void profBegin(int tag, int level, int iters);
   // st: the stream the timed work is queued on (the handle's stream when 0)
-  void profBeginPx(int tag, long long px, int iters, cudaStream_t st = 0);
+  // launches: kernel launches in the group (0: one per iteration)
+  void profBeginPx(int tag, long long px, int iters, cudaStream_t st = 0, int launches = 0);
   void profEnd(cudaStream_t st = 0);
 
  private:

@@ -93,8 +93,15 @@ class StereoTgv:
         check(self._h, self._L.vfs_set_autotune(self._h, int(on)))
 
     def set_iteration_variant(self, variant: int) -> None:
-        """Force one variant (0..5) of the fused iteration kernel, or -1 for the tuned choice."""
+        """Force one variant (0..9) of the fused iteration kernel, or -1 for the tuned choice."""
         check(self._h, self._L.vfs_set_iteration_variant(self._h, int(variant)))
+
+    def iteration_variants(self):
+        """Iteration-kernel variant per pyramid level (finest first) of the last fused solve."""
+        out = (ctypes.c_int * 16)()
+        n = ctypes.c_int()
+        check(self._h, self._L.vfs_get_iteration_variants(self._h, out, 16, ctypes.byref(n)))
+        return [out[i] for i in range(min(n.value, 16))]
 
     # ---- reference methods -------------------------------------------------
     def initialize(self, width, height, beta, gamma, alpha0, alpha1, timestep_lambda, lambda_,
@@ -228,14 +235,14 @@ class StereoTgv:
             raise VfsError(st, L.vfs_last_error(None).decode(errors="replace"))
 
     def profile_intervals(self, kind: int) -> np.ndarray:
-        """(start_ms, end_ms, pixel_iterations) rows of the records of a kind, relative to
-        the last profile_epoch()."""
+        """(start_ms, end_ms, pixel_iterations, launches) rows of the records of a kind,
+        relative to the last profile_epoch()."""
         n = ctypes.c_int()
-        check(self._h, self._L.vfs_profile_intervals(self._h, kind, 0, None, None, None, ctypes.byref(n)))
-        out = np.zeros((3, n.value), np.float64)
+        check(self._h, self._L.vfs_profile_intervals(self._h, kind, 0, None, None, None, None, ctypes.byref(n)))
+        out = np.zeros((4, n.value), np.float64)
         if n.value:
             check(self._h, self._L.vfs_profile_intervals(self._h, kind, n.value, _ptr(out[0]), _ptr(out[1]),
-                                                         _ptr(out[2]), ctypes.byref(n)))
+                                                         _ptr(out[2]), _ptr(out[3]), ctypes.byref(n)))
         return out.T.copy()
 
     def debug_buffer(self, name: str, comps: int = 1) -> np.ndarray:
@@ -291,7 +298,7 @@ class StereoBatch:
         check_batch(self._h, self._L.vfs_batch_set_autotune(self._h, int(on)))
 
     def set_iteration_variant(self, variant: int) -> None:
-        """Force one variant (0..5) of the fused iteration kernel, or -1 for the tuned choice."""
+        """Force one variant (0..9) of the fused iteration kernel, or -1 for the tuned choice."""
         check_batch(self._h, self._L.vfs_batch_set_iteration_variant(self._h, int(variant)))
 
     def set_mode(self, one_launch: bool) -> None:
