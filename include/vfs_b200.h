@@ -172,6 +172,10 @@ int vfs_set_autotune(vfs_stereo* s, int on);
  * this selects speed only.  (No counterpart in the reference.) */
 #define VFS_ITER_VARIANTS 10
 int vfs_set_iteration_variant(vfs_stereo* s, int variant);
+/* Force one variant per pyramid level (finest first; levels beyond n_levels use variant 1),
+ * e.g. to pin a tuned choice; n_levels = 0 clears it. */
+int vfs_set_iteration_variants(vfs_stereo* s, const int* variants, int n_levels);
+int vfs_batch_set_iteration_variants(vfs_batch* b, const int* variants, int n_levels);
 /* The variant each pyramid level (finest first) used in the handle's last fused solve
  * (tuned, default or forced); *count receives the number of levels. */
 int vfs_get_iteration_variants(vfs_stereo* s, int* variants, int max_levels, int* count);

@@ -213,3 +213,22 @@ def test_launch_overlap_does_not_change_results(gpu):
     finally:
         lib().vfs_set_launch_overlap(1)
     assert np.array_equal(out[0], out[2]) and np.array_equal(out[1], out[3])
+
+
+def test_per_level_variants_and_tuned_choice_reported(gpu):
+    """A per-level variant list (here one-iteration at full resolution, five iterations per
+    launch below) gives the drop-in path's bits, and the handle reports what it ran."""
+    i0, i1, mask, tv, cv = random_case(120, 90, seed=808)
+    p = params(n_levels=3, n_warp=2, n_iter=11)
+    ref = make(i0, i1, mask, tv, cv, p, fused=False)
+    solve_frames(ref, i0, i1, True, 2)
+    s = make(i0, i1, mask, tv, cv, p, fused=True)
+    s.set_iteration_variants([1, 9, 8])
+    solve_frames(s, i0, i1, True, 2)
+    assert s.iteration_variants() == [1, 9, 8]
+    for n, c in (("u", 1), ("warpUV", 2), ("Tp", 2)):
+        assert np.array_equal(s.debug_buffer(n, c), ref.debug_buffer(n, c)), n
+    t = make(i0, i1, mask, tv, cv, p, fused=True)
+    solve_frames(t, i0, i1, True, 1)  # autotuned
+    v = t.iteration_variants()
+    assert len(v) == 3 and all(0 <= x < 10 for x in v)

@@ -79,6 +79,8 @@ SIGNATURES = {
     "vfs_set_autotune": [_vp, _i],
     "vfs_set_iteration_variant": [_vp, _i],
     "vfs_get_iteration_variants": [_vp, _vp, _i, ctypes.POINTER(_i)],
+    "vfs_set_iteration_variants": [_vp, _vp, _i],
+    "vfs_batch_set_iteration_variants": [_vp, _vp, _i],
     "vfs_batch_set_iteration_variant": [_vp, _i],
     "vfs_equalize_hist_u8": [_vp, _vp, _sz, _vp],
     "vfs_equalize_hist_u8_noalloc": [_vp, _vp, _sz, _i, _vp],

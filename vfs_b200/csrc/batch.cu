@@ -439,7 +439,8 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   std::vector<int> comp{(int)masked, (int)half, concurrency};
   for (auto& g : geo) comp.insert(comp.end(), g.begin(), g.end());
   auto tit = tuned_.find(comp);
-  if (tit == tuned_.end() && forced_variant >= 0) tit = tuned_.emplace(comp, std::vector<int>(maxL, forced_variant)).first;
+  const bool forced = forced_variant >= 0 || !forced_levels.empty();
+  if (tit == tuned_.end() && forced) tit = tuned_.emplace(comp, std::vector<int>(maxL, kIterDefaultVariant)).first;
   if (tit == tuned_.end()) {
     std::vector<int> lv(maxL, autotune ? -1 : kIterDefaultVariant);
     if (autotune) {
@@ -453,6 +454,10 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   }
   std::vector<int> variants = tit->second;
   if (forced_variant >= 0) variants.assign(maxL, forced_variant);
+  if (!forced_levels.empty()) {
+    variants.assign(maxL, kIterDefaultVariant);
+    for (int l = 0; l < maxL && l < (int)forced_levels.size(); l++) variants[l] = forced_levels[l];
+  }
   last_variants = variants;
   if (!use_graph) {
     fused_solve_direct(pairs, masked, half, st, variants, false, concurrency);

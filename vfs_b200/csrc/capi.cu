@@ -349,6 +349,24 @@ int vfs_set_iteration_variant(vfs_stereo* s, int variant) {
   });
 }
 
+namespace {
+std::vector<int> checked_levels(const int* variants, int n) {
+  if (n < 0 || n > 32 || (n > 0 && !variants)) throw vfs::ArgError{"invalid per-level variant list"};
+  std::vector<int> v(variants, variants + n);
+  for (int x : v)
+    if (x < 0 || x >= vfs::kIterVariants) throw vfs::ArgError{"iteration variant out of range"};
+  return v;
+}
+}  // namespace
+
+int vfs_set_iteration_variants(vfs_stereo* s, const int* variants, int n_levels) {
+  return guarded(s, [&] { s->impl.engine.forced_levels = checked_levels(variants, n_levels); });
+}
+
+int vfs_batch_set_iteration_variants(vfs_batch* b, const int* variants, int n_levels) {
+  return guarded(b, [&] { b->engine.forced_levels = checked_levels(variants, n_levels); });
+}
+
 int vfs_get_iteration_variants(vfs_stereo* s, int* variants, int max_levels, int* count) {
   return guarded(s, [&] {
     const std::vector<int>& v = s->impl.engine.last_variants;
@@ -427,14 +445,17 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
       vfs::FusedEngine& eng = pairs[k]->engine;
       const bool g = eng.use_graph, t = eng.autotune;
       const int fv = eng.forced_variant, cc = eng.concurrency;
+      const std::vector<int> fl = eng.forced_levels;
       eng.use_graph = b->engine.use_graph;
       eng.autotune = b->engine.autotune;
       eng.forced_variant = b->engine.forced_variant;
+      eng.forced_levels = b->engine.forced_levels;
       eng.concurrency = (int)pairs.size();
       auto restore = [&] {
         eng.use_graph = g;
         eng.autotune = t;
         eng.forced_variant = fv;
+        eng.forced_levels = fl;
         eng.concurrency = cc;
       };
       try {

@@ -45,6 +45,7 @@ class FusedEngine {
   bool use_graph = true;
   bool autotune = true;  // pick the iteration kernel's tile variant per level on first use
   int forced_variant = -1;  // >= 0: this iteration-kernel variant at every level (no tuning)
+  std::vector<int> forced_levels;  // non-empty: variant per level, finest first (no tuning)
   int concurrency = 1;      // one-pair solves run at the same time (set by a concurrent batch)
   // tuned tile variant per level, keyed by batch composition (form, storage, sizes)
   const std::map<std::vector<int>, std::vector<int>>& tuned() const { return tuned_; }

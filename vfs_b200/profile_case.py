@@ -4,12 +4,16 @@ unless --autotune 1, so the launch sequence is fixed).
 
     python -m vfs_b200.profile_case --batch 4 --half 1 [--frames 1] [--path fused|plain]
                                     [--mode concurrent|one_launch] [--autotune 0|1]
+                                    [--variant -1..9] [--variants 1,1,8,9,9]
 
 Launch order per frame: pyramid, then per level (coarse to fine) the level kernels and per
-warp the prologue, the 50 fused iterations and the epilogue.  In the concurrent mode each
-pair's solve is enqueued in turn (pair 0 first), so k_fused_iter launches 600..749 are pair
-0's full-resolution iterations (one pair per launch).  In the one-launch mode every launch
-carries all pairs, and launches 600..749 are the full-resolution iterations of the batch.
+warp the prologue, the fused iterations and the epilogue.  With the default iteration
+variant (or --variant 0..5) each warp has 50 one-iteration launches: in the concurrent mode
+each pair's solve is enqueued in turn (pair 0 first), so k_fused_iter launches 600..749 are
+pair 0's full-resolution iterations (one pair per launch); in the one-launch mode every
+launch carries all pairs, and launches 600..749 are the full-resolution iterations of the
+batch.  With --variant 6..9 (K iterations per launch) each warp has 50 / K launches of
+k_fused_iter_tb, coarsest level first.
 """
 from __future__ import annotations
 
@@ -29,6 +33,8 @@ def main():
     ap.add_argument("--height", type=int, default=800)
     ap.add_argument("--mode", default="concurrent", choices=["concurrent", "one_launch"])
     ap.add_argument("--autotune", type=int, default=0)
+    ap.add_argument("--variant", type=int, default=-1, help="force one iteration-kernel variant")
+    ap.add_argument("--variants", default="", help="force a variant per level, finest first, e.g. 1,1,8,9,9")
     a = ap.parse_args()
     from . import synth
     from .stereotgv import StereoBatch, StereoTgv
@@ -47,6 +53,10 @@ def main():
         batch.set_graph(False)
         batch.set_autotune(bool(a.autotune))
         batch.set_mode(one_launch=a.mode == "one_launch")
+        if a.variant >= 0:
+            batch.set_iteration_variant(a.variant)
+        if a.variants:
+            batch.set_iteration_variants([int(v) for v in a.variants.split(",")])
     solvers = []
     for _ in range(a.batch if fused else 1):
         s = StereoTgv()

@@ -96,6 +96,11 @@ class StereoTgv:
         """Force one variant (0..9) of the fused iteration kernel, or -1 for the tuned choice."""
         check(self._h, self._L.vfs_set_iteration_variant(self._h, int(variant)))
 
+    def set_iteration_variants(self, variants) -> None:
+        """Force one variant per pyramid level (finest first); an empty list clears it."""
+        arr = (ctypes.c_int * max(1, len(variants)))(*variants)
+        check(self._h, self._L.vfs_set_iteration_variants(self._h, arr, len(variants)))
+
     def iteration_variants(self):
         """Iteration-kernel variant per pyramid level (finest first) of the last fused solve."""
         out = (ctypes.c_int * 16)()
@@ -300,6 +305,11 @@ class StereoBatch:
     def set_iteration_variant(self, variant: int) -> None:
         """Force one variant (0..9) of the fused iteration kernel, or -1 for the tuned choice."""
         check_batch(self._h, self._L.vfs_batch_set_iteration_variant(self._h, int(variant)))
+
+    def set_iteration_variants(self, variants) -> None:
+        """Force one variant per pyramid level (finest first); an empty list clears it."""
+        arr = (ctypes.c_int * max(1, len(variants)))(*variants)
+        check_batch(self._h, self._L.vfs_batch_set_iteration_variants(self._h, arr, len(variants)))
 
     def set_mode(self, one_launch: bool) -> None:
         """False (default): pairs run concurrently, each from its own CUDA graph; True: one
