@@ -49,6 +49,8 @@ def parse():
                     help="frames: 848x800 batch (headline); mixed: 8x848x800 + 4x640x480 + 4x424x400 in one "
                          "batch; serving: 6 camera streams with Poisson arrivals")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--fine", type=int, default=-1,
+                    help="fused batches: pairs at full resolution at a time (-1 auto, 0 no limit)")
     return ap.parse_args()
 
 
@@ -313,6 +315,7 @@ def run_ours(args, rank, world, local):
     sbatch = None
     if fused:
         sbatch = StereoBatch(half_storage=half, stream=stream)
+        sbatch.set_fine_concurrency(args.fine)
         for s in solvers:
             sbatch.add(s)
     d_imgs = [(torch.from_numpy(p["i0"]).to(dev), torch.from_numpy(p["i1"]).to(dev)) for p in pairs]
@@ -456,6 +459,7 @@ def run_ours(args, rank, world, local):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "848x800 fisheye stereo pairs, masked TGV-L1 solve, 5 levels x 3 warps x 50 iterations",
                        "path": args.path, "batch_per_gpu": batch, "storage": "fp16" if half else "fp32",
+                       "full_resolution_pairs_at_once": "auto" if args.fine < 0 else args.fine,
                        "l2": "flushed (256 MiB write) before every step",
                        "seed": args.seed, "parallelism": f"replicas x{world}"},
             "latency_ms": {"p50": float(np.percentile(per_frame, 50)), "p99": float(np.percentile(per_frame, 99)),
@@ -513,6 +517,7 @@ def run_mixed(args):
     stream = torch.cuda.Stream(device=dev)
     pairs, solvers = [], []
     batch = StereoBatch(half_storage=False, stream=stream)
+    batch.set_fine_concurrency(args.fine)
     for k, (w, h) in enumerate(sizes):
         p = pair_cache(w, h, args.seed + 100 + k)
         s = StereoTgv()
@@ -576,7 +581,8 @@ def run_mixed(args):
         "unit": "frames/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_step,
         "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "8x848x800 + 4x640x480 + 4x424x400 pairs, masked solve, 3 warps x 50 iterations",
-                   "storage": "fp32", "l2": "flushed (256 MiB write) before every step"},
+                   "storage": "fp32", "l2": "flushed (256 MiB write) before every step",
+                   "full_resolution_pairs_at_once": "auto" if args.fine < 0 else args.fine},
         "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
         "max_abs_vs_plain_px": worst,
     }), flush=True)

@@ -232,3 +232,35 @@ def test_per_level_variants_and_tuned_choice_reported(gpu):
     solve_frames(t, i0, i1, True, 1)  # autotuned
     v = t.iteration_variants()
     assert len(v) == 3 and all(0 <= x < 10 for x in v)
+
+
+@pytest.mark.parametrize("fine,stagger,prio", [(1, 0, 0), (2, 0, 2), (2, 1, 1), (3, 1, 0)])
+def test_fine_concurrency_limit_keeps_results(gpu, fine, stagger, prio):
+    """Splitting each pair's solve into coarse levels and a full-resolution part, with at most
+    `fine` pairs at full resolution at a time (optionally with the coarse parts staggered the
+    same way and the full-resolution parts on high-priority streams), gives the same bits as
+    the unsplit batch, over two frames and from host buffers too."""
+    from vfs_b200.stereotgv import StereoBatch
+    cases = [(96, 64, 2), (130, 101, 3), (67, 53, 2), (200, 120, 3)]
+    p0 = params(n_warp=2, n_iter=6)
+    ref_b, lim_b = StereoBatch(half_storage=True), StereoBatch(half_storage=True)
+    lim_b.set_fine_concurrency(fine)
+    lim_b.set_pipeline(bool(stagger), prio)
+    data = []
+    for k, (w, h, L) in enumerate(cases):
+        i0, i1, mask, tv, cv = random_case(w, h, seed=900 + k)
+        p = dict(p0, n_levels=L)
+        ref_b.add(make(i0, i1, mask, tv, cv, p, fused=True, half=True))
+        lim_b.add(make(i0, i1, mask, tv, cv, p, fused=True, half=True))
+        data.append((i0, i1))
+    for frame in range(2):
+        want = ref_b.solve_host(data)
+        if frame == 0:
+            for m, (i0, i1) in zip(lim_b.members, data):
+                m.copyImagesToDevice(i0, i1)
+            lim_b.solve(True)
+            got = [m.copy1DDisparityToHost() for m in lim_b.members]
+        else:
+            got = lim_b.solve_host(data)
+        for k, (g, w_) in enumerate(zip(got, want)):
+            assert np.array_equal(g, w_), (frame, k)

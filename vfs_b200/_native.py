@@ -76,6 +76,8 @@ SIGNATURES = {
     "vfs_batch_solve_host": [_vp, _vp, _vp, _vp, _i],
     "vfs_batch_set_autotune": [_vp, _i],
     "vfs_batch_set_mode": [_vp, _i],
+    "vfs_batch_set_fine_concurrency": [_vp, _i],
+    "vfs_batch_set_pipeline": [_vp, _i, _i],
     "vfs_set_autotune": [_vp, _i],
     "vfs_set_iteration_variant": [_vp, _i],
     "vfs_get_iteration_variants": [_vp, _vp, _i, ctypes.POINTER(_i)],

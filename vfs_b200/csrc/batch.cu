@@ -38,8 +38,11 @@ void set_iter_tiles(IterArgs& A, int k, int w, int h, int rows) {
 // concurrent mode); the tuner's cost of a variant is its time per iteration times the larger
 // of the share of the GPU its launches occupy and 1 / concurrency, so that with several pairs
 // in flight it weighs the GPU time a variant takes from the others, and alone its latency.
+// part: 0 the whole solve; 1 the calibration warp, the pyramid and the levels above full
+// resolution (ending with the upscale to it); 2 the full-resolution level alone.  Running part 1
+// then part 2 enqueues exactly what part 0 does.
 void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st,
-                        std::vector<int>& level_variant, bool can_tune, int concurrency) {
+                        std::vector<int>& level_variant, bool can_tune, int concurrency, int part) {
   const int n = (int)pairs.size();
   if (n == 0) return;
   if (n > kMaxPairs) throw ArgError{"batch larger than " + std::to_string(kMaxPairs) + " pairs"};
@@ -55,6 +58,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   }
   StereoTgvImpl* prof = pairs[0];
   // ---- calibration warp, state reset, image pyramid (stereotgv.cu:392-405) ---------
+  if (part != 2) {
   for (auto* s : pairs) {
     launch_warp_image(s->tex1(s->pI1[0], 0), s->d_cv, s->d_i1calibrated, s->geomAt(0), st);
     std::swap(s->pI1[0], s->d_i1calibrated);
@@ -82,8 +86,10 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     D.npairs = k;
     launch_downscale_batched(D, st);
   }
+  }  // part != 2
   // ---- levels -------------------------------------------------------------------------
   for (int level = maxL - 1; level >= 0; level--) {
+    if ((part == 1 && level == 0) || (part == 2 && level > 0)) continue;
     std::vector<StereoTgvImpl*> act;
     for (auto* s : pairs)
       if (level < s->levels()) act.push_back(s);
@@ -391,6 +397,16 @@ void set_ptrs(StereoTgvImpl* s, const PairPtrs& p) {
 
 FusedEngine::~FusedEngine() { clear(); }
 
+void FusedEngine::note_variants(const std::vector<int>& v, int part) {
+  if (part == 0) {
+    last_variants = v;
+    return;
+  }
+  last_variants.resize(v.size(), -1);
+  for (size_t l = 0; l < v.size(); l++)
+    if ((part == 1 && l > 0) || (part == 2 && l == 0)) last_variants[l] = v[l];
+}
+
 void FusedEngine::clear() {
   for (auto& kv : cache_) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -424,7 +440,7 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
   }
 }
 
-void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st) {
+void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st, int part) {
   if (pairs.empty()) return;
   prepare(pairs, masked);
   // tile variants per level for this batch composition (tuned on its first solve)
@@ -440,17 +456,18 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   for (auto& g : geo) comp.insert(comp.end(), g.begin(), g.end());
   auto tit = tuned_.find(comp);
   const bool forced = forced_variant >= 0 || !forced_levels.empty();
-  if (tit == tuned_.end() && forced) tit = tuned_.emplace(comp, std::vector<int>(maxL, kIterDefaultVariant)).first;
-  if (tit == tuned_.end()) {
-    std::vector<int> lv(maxL, autotune ? -1 : kIterDefaultVariant);
-    if (autotune) {
-      // first solve of this composition: run it directly and tune while it runs
-      fused_solve_direct(pairs, masked, half, st, lv, true, concurrency);
-      tuned_[comp] = lv;
-      last_variants = lv;
-      return;
-    }
-    tit = tuned_.emplace(comp, lv).first;
+  if (tit == tuned_.end())
+    tit = tuned_.emplace(comp, std::vector<int>(maxL, (autotune && !forced) ? -1 : kIterDefaultVariant)).first;
+  bool need_tune = false;
+  for (int l = 0; l < maxL; l++)
+    if (!((part == 1 && l == 0) || (part == 2 && l > 0)) && tit->second[l] < 0) need_tune = true;
+  if (need_tune) {
+    // first solve of this composition (and part): run it directly and tune while it runs
+    std::vector<int> lv = tit->second;
+    fused_solve_direct(pairs, masked, half, st, lv, true, concurrency, part);
+    tit->second = lv;
+    note_variants(lv, part);
+    return;
   }
   std::vector<int> variants = tit->second;
   if (forced_variant >= 0) variants.assign(maxL, forced_variant);
@@ -458,13 +475,13 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     variants.assign(maxL, kIterDefaultVariant);
     for (int l = 0; l < maxL && l < (int)forced_levels.size(); l++) variants[l] = forced_levels[l];
   }
-  last_variants = variants;
+  note_variants(variants, part);
   if (!use_graph) {
-    fused_solve_direct(pairs, masked, half, st, variants, false, concurrency);
+    fused_solve_direct(pairs, masked, half, st, variants, false, concurrency, part);
     return;
   }
   StereoTgvImpl* prof = pairs[0];
-  std::vector<uintptr_t> key{(uintptr_t)masked, (uintptr_t)half, (uintptr_t)prof->profiling};
+  std::vector<uintptr_t> key{(uintptr_t)masked, (uintptr_t)half, (uintptr_t)prof->profiling, (uintptr_t)part};
   for (int v : variants) key.push_back((uintptr_t)v);
   std::vector<PairPtrs> before;
   for (auto* s : pairs) {
@@ -488,7 +505,7 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     long long launches0 = launch_counter().load();
     VFS_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
     try {
-      fused_solve_direct(pairs, masked, half, st, variants, false, concurrency);
+      fused_solve_direct(pairs, masked, half, st, variants, false, concurrency, part);
     } catch (...) {
       prof->capture_events = nullptr;
       cudaGraph_t junk = nullptr;
@@ -514,7 +531,12 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   VFS_CUDA(cudaGraphLaunch(it->second.exec, st));
   launch_counter().fetch_add(it->second.kernels);
   for (size_t k = 0; k < pairs.size(); k++) set_ptrs(pairs[k], it->second.after[k]);
-  if (prof->profiling) prof->setProfRecords(it->second.prof);
+  if (prof->profiling) {
+    // the full-resolution part continues the frame whose coarse part ran just before
+    std::vector<ProfRec> recs = part == 2 ? prof->profRecords() : std::vector<ProfRec>{};
+    recs.insert(recs.end(), it->second.prof.begin(), it->second.prof.end());
+    prof->setProfRecords(recs);
+  }
 }
 
 }  // namespace vfs

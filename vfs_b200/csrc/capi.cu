@@ -21,6 +21,13 @@ struct vfs_batch {
   std::vector<cudaEvent_t> ready;  // member work finished (the batch stream waits on them)
   std::vector<cudaStream_t> lanes;     // concurrent mode: one stream per member slot
   std::vector<cudaEvent_t> lane_done;  // concurrent mode: per-slot completion
+  std::vector<cudaEvent_t> fine_done;  // concurrent mode: per-slot end of the full-resolution part
+  std::vector<cudaEvent_t> coarse_done;  // concurrent mode: per-slot end of the coarse part
+  std::vector<cudaStream_t> fine_lanes;  // concurrent mode: streams of the full-resolution parts
+  int fine_limit = -1;  // concurrent mode: pairs at full resolution at once (0: no limit, -1: auto)
+  bool stagger_coarse = false;  // coarse parts also S at a time, one slot ahead of the fine parts
+  int fine_priority = 0;  // 1: full-resolution parts on high-priority streams; 2: also the
+                          // coarse parts of the first max_pairs pairs
   int mode = VFS_BATCH_CONCURRENT;
   bool half = false;
   std::string err;
@@ -28,6 +35,9 @@ struct vfs_batch {
     engine.clear();
     for (auto e : ready) cudaEventDestroy(e);
     for (auto e : lane_done) cudaEventDestroy(e);
+    for (auto e : fine_done) cudaEventDestroy(e);
+    for (auto e : coarse_done) cudaEventDestroy(e);
+    for (auto l : fine_lanes) cudaStreamDestroy(l);
     for (auto l : lanes) cudaStreamDestroy(l);
     if (done) cudaEventDestroy(done);
     if (start) cudaEventDestroy(start);
@@ -382,6 +392,21 @@ int vfs_batch_set_iteration_variant(vfs_batch* b, int variant) {
   });
 }
 
+int vfs_batch_set_fine_concurrency(vfs_batch* b, int max_pairs) {
+  return guarded(b, [&] {
+    if (max_pairs < -1) throw vfs::ArgError{"fine concurrency must be >= -1"};
+    b->fine_limit = max_pairs;
+  });
+}
+
+int vfs_batch_set_pipeline(vfs_batch* b, int stagger_coarse, int priority) {
+  return guarded(b, [&] {
+    if (priority < 0 || priority > 2) throw vfs::ArgError{"pipeline priority must be 0, 1 or 2"};
+    b->stagger_coarse = stagger_coarse != 0;
+    b->fine_priority = priority;
+  });
+}
+
 int vfs_batch_set_mode(vfs_batch* b, int mode) {
   return guarded(b, [&] {
     if (mode != VFS_BATCH_CONCURRENT && mode != VFS_BATCH_ONE_LAUNCH) throw vfs::ArgError{"unknown batch mode"};
@@ -436,11 +461,35 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
       cudaEvent_t e;
       VFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
       b->lane_done.push_back(e);
+      VFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      b->fine_done.push_back(e);
+      VFS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      b->coarse_done.push_back(e);
+      int lo = 0, hi = 0;  // numerically lower priority values are higher priorities
+      VFS_CUDA(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+      VFS_CUDA(cudaStreamCreateWithPriority(&l, cudaStreamNonBlocking, hi));
+      b->fine_lanes.push_back(l);
     }
-    VFS_CUDA(cudaEventRecord(b->start, b->stream));
-    for (size_t k = 0; k < pairs.size(); k++) {
-      VFS_CUDA(cudaStreamWaitEvent(b->lanes[k], b->start, 0));
-      if (io) pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], cudaMemcpyHostToDevice, b->lanes[k]);
+    const int n = (int)pairs.size();
+    // With a limit S on the pairs at full resolution, each pair's solve is enqueued as two
+    // graphs: the coarse levels of every pair start together, and pair k's full-resolution
+    // level waits for pair k - S's, so that at most S full-resolution working sets compete
+    // for L2 while the other pairs run their coarse levels.
+    int S = b->fine_limit;
+    if (S < 0) {
+      // auto: as many full-resolution working sets as fit in three quarters of L2, at least
+      // two (per pixel: the iteration's reads and the other ping-pong planes it writes)
+      int dev = 0, l2 = 0;
+      VFS_CUDA(cudaGetDevice(&dev));
+      VFS_CUDA(cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, dev));
+      double ws = 0;
+      for (auto* p : pairs) ws = std::max(ws, (double)p->width * p->height * (b->half ? 69.0 : 101.0));
+      // no split when fewer than two working sets fit (the limit then only serialises)
+      S = ws > 0 ? (int)(0.75 * l2 / ws) : 0;
+      if (S < 2) S = 0;
+    }
+    const bool split = S > 0 && S < n;
+    auto run = [&](int k, int part, int concurrency, cudaStream_t lane) {
       std::vector<vfs::StereoTgvImpl*> one{pairs[k]};
       vfs::FusedEngine& eng = pairs[k]->engine;
       const bool g = eng.use_graph, t = eng.autotune;
@@ -450,7 +499,7 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
       eng.autotune = b->engine.autotune;
       eng.forced_variant = b->engine.forced_variant;
       eng.forced_levels = b->engine.forced_levels;
-      eng.concurrency = (int)pairs.size();
+      eng.concurrency = concurrency;
       auto restore = [&] {
         eng.use_graph = g;
         eng.autotune = t;
@@ -459,15 +508,46 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
         eng.concurrency = cc;
       };
       try {
-        eng.solve(one, masked != 0, b->half, b->lanes[k]);
+        eng.solve(one, masked != 0, b->half, lane, part);
       } catch (...) {
         restore();
         throw;
       }
       restore();
+    };
+    VFS_CUDA(cudaEventRecord(b->start, b->stream));
+    for (int k = 0; k < n; k++) {
+      VFS_CUDA(cudaStreamWaitEvent(b->lanes[k], b->start, 0));
+      // staggered coarse parts: pair k's coarse levels follow pair k - S's
+      if (split && b->stagger_coarse && k >= S) VFS_CUDA(cudaStreamWaitEvent(b->lanes[k], b->coarse_done[k - S], 0));
+      // the first S pairs' coarse parts on the high-priority streams (their full-resolution
+      // parts follow there), so that full-resolution work starts early
+      cudaStream_t cl = (split && b->fine_priority >= 2 && k < S) ? b->fine_lanes[k] : b->lanes[k];
+      if (cl != b->lanes[k]) VFS_CUDA(cudaStreamWaitEvent(cl, b->start, 0));
+      if (io) pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], cudaMemcpyHostToDevice, cl);
+      run(k, split ? 1 : 0, n, cl);
+      if (split) {
+        VFS_CUDA(cudaEventRecord(b->coarse_done[k], cl));
+        continue;
+      }
       if (io) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, b->lanes[k]);
       VFS_CUDA(cudaEventRecord(b->lane_done[k], b->lanes[k]));
       VFS_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
+    }
+    if (split) {
+      for (int k = 0; k < n; k++) {
+        cudaStream_t fl = b->fine_priority ? b->fine_lanes[k] : b->lanes[k];
+        VFS_CUDA(cudaStreamWaitEvent(fl, b->coarse_done[k], 0));
+        if (k >= S) VFS_CUDA(cudaStreamWaitEvent(fl, b->fine_done[k - S], 0));
+        run(k, 2, S, fl);
+        VFS_CUDA(cudaEventRecord(b->fine_done[k], fl));
+        if (io) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, fl);
+        VFS_CUDA(cudaEventRecord(b->lane_done[k], fl));
+        VFS_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
+        // the next solve's parts of this slot follow this one's end
+        VFS_CUDA(cudaStreamWaitEvent(b->lanes[k], b->lane_done[k], 0));
+        VFS_CUDA(cudaStreamWaitEvent(b->fine_lanes[k], b->lane_done[k], 0));
+      }
     }
   }
   VFS_CUDA(cudaEventRecord(b->done, b->stream));

@@ -51,12 +51,14 @@ class FusedEngine {
   const std::map<std::vector<int>, std::vector<int>>& tuned() const { return tuned_; }
   ~FusedEngine();
   void clear();
-  void solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st);
+  // part: 0 whole solve; 1 everything before the full-resolution level; 2 that level alone
+  void solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st, int part = 0);
   // allocate fused buffers and refresh edge codes, each on the pair's own stream
   static void prepare(std::vector<StereoTgvImpl*>& pairs, bool masked);
   size_t graphs() const { return cache_.size(); }
   // iteration-kernel variant per pyramid level (finest first) of the last solve
   std::vector<int> last_variants;
+  void note_variants(const std::vector<int>& v, int part);
 
  private:
   struct Entry {

@@ -99,6 +99,9 @@ class StereoServer:
             b = StereoBatch(half_storage=half_storage)
             b.set_graph(use_graph)
             b.set_autotune(False)  # no timing passes (host synchronisations) inside the serving loop
+            # latency first: every request of a batch runs its full-resolution level at once
+            # (a full-resolution limit raises throughput but delays the later pairs of a batch)
+            b.set_fine_concurrency(0)
             st = torch.cuda.Stream(device=self.device)
             b.set_stream(st)
             self.lanes.append(_Lane(stream=st, batch=b))

@@ -316,6 +316,15 @@ class StereoBatch:
         launch per step and level covers all pairs."""
         check_batch(self._h, self._L.vfs_batch_set_mode(self._h, int(one_launch)))
 
+    def set_fine_concurrency(self, max_pairs: int) -> None:
+        """Concurrent mode: at most max_pairs pairs at full resolution at a time (0: no limit)."""
+        check_batch(self._h, self._L.vfs_batch_set_fine_concurrency(self._h, int(max_pairs)))
+
+    def set_pipeline(self, stagger_coarse: bool, priority: int) -> None:
+        """With a full-resolution limit: stagger the coarse levels too; priority 1 runs the
+        full-resolution parts on high-priority streams, 2 also the first pairs' coarse levels."""
+        check_batch(self._h, self._L.vfs_batch_set_pipeline(self._h, int(stagger_coarse), int(priority)))
+
     def add(self, solver: "StereoTgv") -> None:
         check_batch(self._h, self._L.vfs_batch_add(self._h, solver.handle))
         self.members.append(solver)
