@@ -385,12 +385,9 @@ def run_ours(args, rank, world, local):
     ms_l = union_ms(top[:, :2]) if len(top) else 0.0
     ms_sum = float((top[:, 1] - top[:, 0]).sum()) if len(top) else 0.0
     variants = solvers[0].iteration_variants() if fused else []
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
-    frames = batch * args.steps * world
-    value = frames / (total_ms / 1000.0)
+    # job-wide: frames of all replicas over the slowest replica's time
+    from vfs_b200.replicas import job_rate
+    frames, total_ms, value = job_rate(batch * args.steps, total_ms, device=dev)
 
     # ---- e2e: the public API with pinned host buffers -----------------------------------
     pinned = []  # page-locked host buffers (kept alive for the numpy views)
@@ -431,12 +428,7 @@ def run_ours(args, rank, world, local):
         t0 = time.perf_counter()
         outs = host_step()
         e2e_ms.append(1000 * (time.perf_counter() - t0))
-    e2e_total = float(sum(e2e_ms))
-    if world > 1:
-        t = torch.tensor([e2e_total], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = batch * e2e_steps * world / (e2e_total / 1000.0)
+    _, e2e_total, e2e_value = job_rate(batch * e2e_steps, float(sum(e2e_ms)), device=dev)
     gpu_u = np.array(outs[0])
 
     result = None

@@ -146,8 +146,8 @@ def test_batch_solve_host_matches_device_path(gpu, one_launch):
 @pytest.mark.parametrize("masked", [True, False])
 def test_every_iteration_variant_bit_identical(gpu, masked):
     """All variants of the fused iteration kernel (shared-memory tiles of 4 / 8 / 16 rows,
-    row-streaming strips of 8 / 16 / 32 rows, and 3 or 5 iterations per launch on tiles held
-    in shared memory) give the drop-in path's bits with float storage and one another's bits
+    row-streaming strips of 8 / 16 / 32 rows, 3 or 5 iterations per launch on tiles held in
+    shared memory, two pixels per thread on 62-column tiles) give the drop-in path's bits with float storage and one another's bits
     with half storage, on sizes that cut tiles unevenly.  7 iterations per warp leave a
     remainder after the multi-iteration launches.  The 64 x 48 case has no row padding at
     level 0 and an all-on mask, where the multi-iteration kernel must fall back."""
@@ -161,7 +161,7 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
         solve_frames(ref, i0, i1, masked, 2)
         want = {n: ref.debug_buffer(n, c) for n, c in (("u", 1), ("u_", 1), ("warpUV", 2), ("Tp", 2))}
         half_ref = None
-        for variant in range(10):
+        for variant in range(12):
             s = make(i0, i1, mask, tv, cv, p, fused=True)
             s.set_iteration_variant(variant)
             solve_frames(s, i0, i1, masked, 2)

@@ -246,6 +246,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             if (v >= kIterFirstRowsVariant && v < kIterFirstTBVariant) continue;
             const int kv = tb_iterations(v);
             if (kv > 1 && (!tb_here || kv > P0.nSolverIters)) continue;
+            if (iter_variant_single_pair(v) && na != 1) continue;
             IterArgs T = iter_args(kv > 1 ? kIterDefaultVariant : v, 1.0f, 1.0f, mu0, 0);
             IterTBArgs TB = tb_args(1.0f, 1.0f, 0, kv);
             auto once = [&] {
@@ -279,7 +280,9 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
       // K iterations per launch where the variant is a multi-iteration one and it applies
       // here; the remaining iterations (and the fallback) use the default one-iteration form
       const int K = tb_here ? tb_iterations(variant) : 1;
-      const int v1 = tb_iterations(variant) > 1 ? kIterDefaultVariant : variant;
+      const int v1 = (tb_iterations(variant) > 1 || (iter_variant_single_pair(variant) && na != 1))
+                         ? kIterDefaultVariant
+                         : variant;
       float tau = 1.0f;
       float sigma = 1.0f / tau;
       const int n_it = P0.nSolverIters;

@@ -132,6 +132,9 @@ int tb_iterations(int variant);
 double iteration_gpu_share(int variant, bool masked, bool half, int w, int h);
 double rows_gpu_share(int variant, bool masked, bool half, int w, int h);
 double tb_gpu_share(int variant, bool masked, bool half, int w, int h);
+double x2_gpu_share(int variant, bool masked, bool half, int w, int h);
+void launch_fused_iteration_x2(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
+                               int variant);
 void launch_fused_iteration_tb(const IterTBArgs& A, bool masked, bool half_storage, cudaStream_t st, int variant);
 
 // ---- per-warp prologue: zero p, q, v-bar; resample tv at x + warpUV; warp I1 ----
@@ -244,11 +247,16 @@ inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFT
 // variants 6-9: k_fused_iter_tb, several iterations per launch with the tile's region in
 // shared memory (kernels_tb.cu), one pair per launch only: 3 iterations on 64 x 24 tiles,
 // 5 on 32 x 24, and with one region pixel per thread 3 on 23 x 23 and 5 on 17 x 17 tiles.
-constexpr int kIterVariants = 10;
-constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17};
-constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0};
+// variants 10-11: k_fused_iter_x2, two horizontally adjacent pixels per thread on 62 x 8 /
+// 62 x 4 tiles (kernels_x2.cu); one pair per launch only.
+constexpr int kIterVariants = 12;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17, 8, 4};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 3, 6};
 constexpr int kIterFirstRowsVariant = 3;
 constexpr int kIterFirstTBVariant = 6;
+constexpr int kIterFirstX2Variant = 10;
+// variants whose launch carries one pair only (others fall back to the default there)
+inline bool iter_variant_single_pair(int v) { return v >= kIterFirstTBVariant; }
 constexpr int kIterDefaultVariant = 1;
 inline int iter_tiles_x_of(int w) { return (w + 30) / 31; }
 inline int iter_tiles_of(int w, int h, int rows) { return iter_tiles_x_of(w) * ((h + rows - 1) / rows); }

@@ -270,7 +270,9 @@ double iteration_gpu_share(int variant, bool masked, bool half, int w, int h) {
   // blocks of the launch and resident blocks per SM of the variant's kernel (one pair)
   long long blocks = 0;
   int per_sm = 0;
-  if (variant >= kIterFirstTBVariant) {
+  if (variant >= kIterFirstX2Variant) {
+    return x2_gpu_share(variant, masked, half, w, h);
+  } else if (variant >= kIterFirstTBVariant) {
     return tb_gpu_share(variant, masked, half, w, h);
   } else if (variant >= kIterFirstRowsVariant) {
     return rows_gpu_share(variant, masked, half, w, h);
@@ -296,6 +298,10 @@ void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, c
   static_assert(kIterVariantRows[0] == 4 && kIterVariantRows[1] == 8 && kIterVariantRows[2] == 16, "variants");
   if (variant >= kIterFirstRowsVariant && variant < kIterFirstTBVariant) {
     launch_fused_iteration_rows(A, masked, half_storage, st, parity, kIterVariantRows[variant]);
+    return;
+  }
+  if (variant >= kIterFirstX2Variant && variant < kIterVariants) {
+    launch_fused_iteration_x2(A, masked, half_storage, st, parity, variant);
     return;
   }
   switch (variant) {
