@@ -484,7 +484,8 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     return;
   }
   StereoTgvImpl* prof = pairs[0];
-  std::vector<uintptr_t> key{(uintptr_t)masked, (uintptr_t)half, (uintptr_t)prof->profiling, (uintptr_t)part};
+  std::vector<uintptr_t> key{(uintptr_t)masked, (uintptr_t)half, (uintptr_t)prof->profiling, (uintptr_t)part,
+                             (uintptr_t)(intptr_t)launch_priority()};
   for (int v : variants) key.push_back((uintptr_t)v);
   std::vector<PairPtrs> before;
   for (auto* s : pairs) {

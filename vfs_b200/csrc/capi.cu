@@ -489,7 +489,14 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
       if (S < 2) S = 0;
     }
     const bool split = S > 0 && S < n;
-    auto run = [&](int k, int part, int concurrency, cudaStream_t lane) {
+    int prio_lo = 0, prio_hi = 0;
+    VFS_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    auto run = [&](int k, int part, int concurrency, cudaStream_t lane, bool high = false) {
+      struct PrioScope {  // the launches of this part carry the high priority
+        int old;
+        PrioScope(int p) : old(vfs::launch_priority()) { vfs::launch_priority() = p; }
+        ~PrioScope() { vfs::launch_priority() = old; }
+      } prio_scope(high ? prio_hi : 0);
       std::vector<vfs::StereoTgvImpl*> one{pairs[k]};
       vfs::FusedEngine& eng = pairs[k]->engine;
       const bool g = eng.use_graph, t = eng.autotune;
@@ -525,7 +532,7 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
       cudaStream_t cl = (split && b->fine_priority >= 2 && k < S) ? b->fine_lanes[k] : b->lanes[k];
       if (cl != b->lanes[k]) VFS_CUDA(cudaStreamWaitEvent(cl, b->start, 0));
       if (io) pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], cudaMemcpyHostToDevice, cl);
-      run(k, split ? 1 : 0, n, cl);
+      run(k, split ? 1 : 0, n, cl, cl != b->lanes[k]);
       if (split) {
         VFS_CUDA(cudaEventRecord(b->coarse_done[k], cl));
         continue;
@@ -539,7 +546,7 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
         cudaStream_t fl = b->fine_priority ? b->fine_lanes[k] : b->lanes[k];
         VFS_CUDA(cudaStreamWaitEvent(fl, b->coarse_done[k], 0));
         if (k >= S) VFS_CUDA(cudaStreamWaitEvent(fl, b->fine_done[k - S], 0));
-        run(k, 2, S, fl);
+        run(k, 2, S, fl, b->fine_priority >= 1);
         VFS_CUDA(cudaEventRecord(b->fine_done[k], fl));
         if (io) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, fl);
         VFS_CUDA(cudaEventRecord(b->lane_done[k], fl));

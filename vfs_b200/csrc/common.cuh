@@ -55,6 +55,10 @@ struct ArgError {
 // previous launch has completed and its writes are visible, so results do not depend on the
 // overlap.  Process-wide switch (vfs_set_launch_overlap), on by default.
 std::atomic<bool>& pdl_enabled();
+// Scheduling priority given to the fused iteration kernels launched by this host thread (0:
+// none; otherwise a stream-priority value, numerically lower = higher priority).  Set around
+// the launches of the work that should win the block scheduler (kept in captured graphs).
+int& launch_priority();
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void griddep_launch_dependents() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
@@ -62,7 +66,9 @@ __device__ __forceinline__ void griddep_launch_dependents() {
 template <typename... KArgs, typename... Args>
 inline void launch_overlapped_smem(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
                                    Args... args) {
-  if (!pdl_enabled().load(std::memory_order_relaxed)) {
+  const bool pdl = pdl_enabled().load(std::memory_order_relaxed);
+  const int prio = launch_priority();
+  if (!pdl && prio == 0) {
     k<<<grid, block, smem, st>>>(args...);
     return;
   }
@@ -71,11 +77,20 @@ inline void launch_overlapped_smem(void (*k)(KArgs...), dim3 grid, dim3 block, s
   cfg.blockDim = block;
   cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchAttribute at[2];
+  unsigned n = 0;
+  if (pdl) {
+    at[n].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[n].val.programmaticStreamSerializationAllowed = 1;
+    n++;
+  }
+  if (prio != 0) {
+    at[n].id = cudaLaunchAttributePriority;
+    at[n].val.priority = prio;
+    n++;
+  }
   cfg.attrs = at;
-  cfg.numAttrs = 1;
+  cfg.numAttrs = n;
   VFS_CUDA(cudaLaunchKernelEx(&cfg, k, args...));
 }
 template <typename... KArgs, typename... Args>

@@ -30,6 +30,11 @@ std::atomic<bool>& pdl_enabled() {
   return on;
 }
 
+int& launch_priority() {
+  static thread_local int p = 0;
+  return p;
+}
+
 cudaEvent_t StereoTgvImpl::profEvent() {
   if (capture_events) {
     cudaEvent_t e;
