@@ -264,3 +264,25 @@ def test_fine_concurrency_limit_keeps_results(gpu, fine, stagger, prio):
             got = lim_b.solve_host(data)
         for k, (g, w_) in enumerate(zip(got, want)):
             assert np.array_equal(g, w_), (frame, k)
+
+
+def test_fp16_batch_accuracy_at_full_size(gpu):
+    """The batched FP16-storage form at 848 x 800 (two seeded pairs, autotuned kernels, the
+    default full-resolution schedule) against the FP64 oracle: mean |du| <= 0.05 px and fewer
+    than 1 % of in-mask pixels off by more than 1 px."""
+    from vfs_b200 import synth
+    from vfs_b200.stereotgv import StereoBatch
+    sp = synth.SOLVER_PARAMS
+    p = params(beta=sp["beta"], gamma=sp["gamma"], n_levels=synth.n_levels_for(848), n_warp=sp["nWarpIters"],
+               n_iter=sp["nSolverIters"], limit_range=synth.LIMIT_RANGE)
+    pairs = [synth.make_pair(848, 800, seed=4242 + k) for k in range(2)]
+    b = StereoBatch(half_storage=True)
+    for pr in pairs:
+        b.add(make(pr.i0, pr.i1, pr.mask, pr.tv, pr.cv, p, fused=True, half=True))
+    outs = b.solve_host([(pr.i0, pr.i1) for pr in pairs])
+    for pr, u in zip(pairs, outs):
+        o = run_oracle(pr.i0, pr.i1, pr.mask, pr.tv, pr.cv, p, True, precision=64)
+        m = pr.mask > 0
+        d = np.abs(np.asarray(u, np.float64) - o.get("u"))[m]
+        assert d.mean() <= 0.05, d.mean()
+        assert (d > 1.0).mean() < 0.01
