@@ -121,8 +121,9 @@ int vfs_set_graph(vfs_stereo* s, int use_graph);
 size_t vfs_estimate_device_bytes(int width, int height, int nLevels, float fScale, int strideAlignment,
                                  int fused);
 
-/* Batched solves: several handles (pairs, possibly of different sizes) solved together,
- * one launch per step and pyramid level for all of them, replayed as a CUDA graph.
+/* Batched solves: several handles (pairs, possibly of different sizes) solved together by
+ * the fused path, replayed from CUDA graphs (see vfs_batch_set_mode for how the pairs share
+ * launches).
  * Pairs of a batch need equal nWarpIters, nSolverIters and timestep_lambda.  The batch
  * does not own the handles; vfs_batch_add moves the handle onto the batch's stream.  At
  * most VFS_BATCH_MAX pairs. */

@@ -1,9 +1,10 @@
 // Fused, batched kernels of the fast solve path.
 //
-// One launch covers every pair of a batch at one pyramid level; pairs may differ in
-// size.  Per-pair state is passed by value in the kernel parameters (up to
-// kMaxPairs pairs), with the pointers that are current at that launch, so a launch
-// sequence can be captured once in a CUDA graph and replayed.
+// A launch covers one pair (the batch's concurrent mode, and single solves) or every pair
+// of a batch at one pyramid level (its one-launch mode); pairs may differ in size.
+// Per-pair state is passed by value in the kernel parameters (up to kMaxPairs pairs), with
+// the pointers that are current at that launch, so a launch sequence can be captured once
+// in a CUDA graph and replayed.
 //
 // With float storage the fused kernels compute bit-for-bit what the per-kernel
 // drop-in path computes: the same operations in the same order on the same

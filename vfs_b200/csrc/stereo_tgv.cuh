@@ -26,7 +26,7 @@ struct SolverParams {
 // Which implementation runs the solve.
 enum class SolvePath {
   kReference = 0,  // one kernel per reference kernel (drop-in form)
-  kFused = 1,      // fused kernels with temporal blocking
+  kFused = 1,      // fused kernels (one or several iterations per launch), CUDA graphs
 };
 
 class StereoTgvImpl;
