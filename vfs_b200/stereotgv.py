@@ -265,8 +265,7 @@ class StereoBatch:
     """Several :class:`StereoTgv` pairs solved together by the fused path: by default each
     pair replays its own CUDA graph on one of the batch's streams (the pairs run concurrently,
     at most an L2-sized number of them at full resolution at a time); ``set_mode(True)``
-    makes one launch per step and level cover every pair."""Several :class:`StereoTgv` pairs solved together by the fused path (one launch per step
-    and level for all pairs, replayed as a CUDA graph)."""
+    makes one launch per step and level cover every pair."""
 
     def __init__(self, half_storage: bool = False, stream=None):
         self._L = lib()
