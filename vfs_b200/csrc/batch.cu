@@ -205,6 +205,23 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
           set_iter_tiles(A, k, d.w, d.h, kIterVariantRows[variant]);
         }
         A.npairs = na;
+        A.span_rows = 0;
+        if (na == 1 && masked && variant >= 0 && variant < 3) {
+          const StereoTgvImpl* s = act[0];
+          if (level < (int)s->span_lo[variant].size()) {
+            const std::vector<uint16_t>& lo = s->span_lo[variant][level];
+            const std::vector<uint16_t>& hi = s->span_hi[variant][level];
+            if (!lo.empty() && (int)lo.size() <= kMaxSpanRows) {
+              A.span_rows = (int)lo.size();
+              A.span_max = 0;
+              for (size_t r = 0; r < lo.size(); r++) {
+                A.span_lo[r] = lo[r];
+                A.span_hi[r] = hi[r];
+                if (hi[r] >= lo[r]) A.span_max = std::max(A.span_max, (int)hi[r] - (int)lo[r] + 1);
+              }
+            }
+          }
+        }
         return A;
       };
       // the K-iterations-per-launch kernel: one pair per launch, and exact at this level
@@ -429,14 +446,51 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
       // the multi-iteration kernel cannot follow that pixel, so it is used there only when
       // no pixel of column 0 is on
       s->tb_ok.assign(s->levels(), 1);
+      for (int v = 0; v < 3; v++) {
+        s->span_lo[v].assign(s->levels(), {});
+        s->span_hi[v].assign(s->levels(), {});
+      }
       for (int l = 0; l < s->levels(); l++) {
-        if (s->pW[l] != s->pS[l]) continue;
-        std::vector<uint8_t> col(s->pH[l]);
-        VFS_CUDA(cudaMemcpy2DAsync(col.data(), 1, s->code_masked[l], s->pS[l], 1, s->pH[l], cudaMemcpyDeviceToHost,
+        const int w = s->pW[l], h = s->pH[l];
+        std::vector<uint8_t> code((size_t)w * h);
+        VFS_CUDA(cudaMemcpy2DAsync(code.data(), w, s->code_masked[l], s->pS[l], w, h, cudaMemcpyDeviceToHost,
                                    s->stream()));
         VFS_CUDA(cudaStreamSynchronize(s->stream()));
-        for (uint8_t c : col)
-          if (c & kOn) s->tb_ok[l] = 0;
+        if (w == s->pS[l])
+          for (int y = 0; y < h; y++)
+            if (code[(size_t)y * w] & kOn) s->tb_ok[l] = 0;
+        // first and last on column of every image row
+        std::vector<int> xmin(h, w), xmax(h, -1);
+        for (int y = 0; y < h; y++)
+          for (int x = 0; x < w; x++)
+            if (code[(size_t)y * w + x] & kOn) {
+              xmin[y] = std::min(xmin[y], x);
+              xmax[y] = std::max(xmax[y], x);
+            }
+        const int tiles_x = iter_tiles_x_of(w);
+        for (int v = 0; v < 3; v++) {
+          const int TH = kIterVariantRows[v];
+          const int rows = (h + TH - 1) / TH;
+          std::vector<uint16_t> lo(rows), hi(rows);
+          for (int r = 0; r < rows; r++) {
+            // tile row r covers image rows TH r - 1 (north halo) .. TH r + TH - 1; a column x
+            // lies in tile x / 31 and, when x % 31 == 30, in the west halo of the next tile
+            int a = w, b = -1;
+            for (int y = std::max(0, TH * r - 1); y <= std::min(h - 1, TH * r + TH - 1); y++) {
+              a = std::min(a, xmin[y]);
+              b = std::max(b, xmax[y]);
+            }
+            if (b < 0) {
+              lo[r] = 1;
+              hi[r] = 0;
+              continue;
+            }
+            lo[r] = (uint16_t)(a / 31);
+            hi[r] = (uint16_t)std::min(tiles_x - 1, b / 31 + (b % 31 == 30 ? 1 : 0));
+          }
+          s->span_lo[v][l] = lo;
+          s->span_hi[v][l] = hi;
+        }
       }
       s->codes_valid = true;
     }

@@ -103,12 +103,18 @@ struct IterPair {
   int w, h, s, tiles_x, tile0;
   float alpha0, alpha1, lambda;
 };
+constexpr int kMaxSpanRows = 256;
 struct IterArgs {
   int npairs, ntiles;
   float sigma, tau, mu;
   float sp[kMaxPairs], sq[kMaxPairs];  // alpha1 sigma / 3 and alpha0 sigma / 2 per pair (host-evaluated)
   int write_tp;
   IterPair pr[kMaxPairs];
+  // One-pair masked launches of k_fused_iter: with span_rows > 0 the grid covers, in tile row
+  // r, only the tile columns span_lo[r] .. span_hi[r] (the tiles whose region holds a pixel
+  // that is on); the others would write nothing.  span_max: the widest span (grid width).
+  int span_rows, span_max;
+  uint16_t span_lo[kMaxSpanRows], span_hi[kMaxSpanRows];
 };
 // parity selects which half of the p / q ping-pong buffers is read (the other is written);
 // variant selects the tile height (kIterVariantRows[variant] rows of 31 pixels).

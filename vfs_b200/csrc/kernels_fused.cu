@@ -111,7 +111,12 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   const IterPair& P = A.pr[pi_];
   int x0, y0;
   if (SINGLE) {
-    x0 = (int)blockIdx.x * 31;
+    int tx = (int)blockIdx.x;
+    if (MASKED && A.span_rows > 0) {  // only the tiles of this row that hold a pixel that is on
+      tx += A.span_lo[blockIdx.y];
+      if (tx > (int)A.span_hi[blockIdx.y]) return;
+    }
+    x0 = tx * 31;
     y0 = (int)blockIdx.y * TH;
   } else {
     const int lt_ = t_ - P.tile0;
@@ -234,7 +239,13 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
 template <int TH, int MINB, bool SINGLE>
 static void launch_iter_th2(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity) {
   dim3 blk(32, TH + 1), grid(A.ntiles);
-  if (SINGLE) grid = dim3(A.pr[0].tiles_x, (A.pr[0].h + TH - 1) / TH);
+  if (SINGLE) {
+    grid = dim3(A.pr[0].tiles_x, (A.pr[0].h + TH - 1) / TH);
+    if (masked && A.span_rows > 0) {
+      if (A.span_rows != (int)grid.y) throw ArgError{"tile spans do not match the launch"};
+      grid.x = A.span_max > 0 ? A.span_max : 1;
+    }
+  }
   if (masked) {
     if (half_storage) launch_overlapped(k_fused_iter<true, __half, TH, MINB, SINGLE>, grid, blk, st, A, parity);
     else launch_overlapped(k_fused_iter<true, float, TH, MINB, SINGLE>, grid, blk, st, A, parity);
