@@ -385,6 +385,7 @@ def run_ours(args, rank, world, local):
     ms_l = union_ms(top[:, :2]) if len(top) else 0.0
     ms_sum = float((top[:, 1] - top[:, 0]).sum()) if len(top) else 0.0
     variants = solvers[0].iteration_variants() if fused else []
+    n_variant_sets = len({tuple(s.iteration_variants()) for s in solvers}) if fused else 0
     # job-wide: frames of all replicas over the slowest replica's time
     from vfs_b200.replicas import job_rate
     frames, total_ms, value = job_rate(batch * args.steps, total_ms, device=dev)
@@ -469,6 +470,7 @@ def run_ours(args, rank, world, local):
                          "all_levels": {"achieved": achieved_all, "frac": (achieved_all / peak) if achieved_all else None,
                                         "busy_ms": ms_all},
                          "iteration_variants_by_level": variants,
+                         "distinct_variant_choices_over_pairs": n_variant_sets,
                          "traffic_source": "profiles/roofline_traffic.json (ncu) x pixels per launch"
                          if traffic is not None else None},
             "e2e": {"value": e2e_value, "unit": "frames/s", "h2d_bytes_per_step": batch * 2 * W0 * H0,

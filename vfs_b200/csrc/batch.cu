@@ -7,6 +7,7 @@
 #include <array>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "fused.cuh"
@@ -257,6 +258,10 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
           cudaEvent_t e0, e1;
           VFS_CUDA(cudaEventCreate(&e0));
           VFS_CUDA(cudaEventCreate(&e1));
+          // two passes over the candidates, each keeping its faster pass, so that one
+          // disturbed measurement (other pairs' work on the GPU) does not decide the level
+          std::vector<float> best_ms(kIterVariants, 1e30f);
+          for (int pass = 0; pass < 2; pass++)
           for (int v = 0; v < kIterVariants; v++) {
             // the row-streaming forms are slower everywhere on B200 (one warp walks its strip
             // serially); they stay available as forced variants
@@ -278,9 +283,14 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             float ms = 0;
             VFS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
             ms /= (float)kv;  // per iteration
+            best_ms[v] = std::min(best_ms[v], ms);
+            if (pass == 0) continue;
+            ms = best_ms[v];
             double share = 1.0;
             if (na == 1) share = iteration_gpu_share(v, masked, half, act[0]->pW[level], act[0]->pH[level]);
-            const double cost = (double)ms * std::max(share, floor_share);
+            double cost = (double)ms * std::max(share, floor_share);
+            // the default keeps its place unless another variant is clearly (5 %) cheaper
+            if (v == kIterDefaultVariant) cost *= 0.95;
             if (cost < best) {
               best = cost;
               best_v = v;
@@ -415,6 +425,16 @@ void set_ptrs(StereoTgvImpl* s, const PairPtrs& p) {
   s->f_vhs = p.vhs;
 }
 
+// Tuned choices shared by every engine of the process, keyed like FusedEngine::tuned_.
+std::map<std::vector<int>, std::vector<int>>& shared_tuned() {
+  static std::map<std::vector<int>, std::vector<int>> m;
+  return m;
+}
+std::mutex& shared_tuned_mutex() {
+  static std::mutex m;
+  return m;
+}
+
 FusedEngine::~FusedEngine() { clear(); }
 
 void FusedEngine::note_variants(const std::vector<int>& v, int part) {
@@ -515,14 +535,32 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   const bool forced = forced_variant >= 0 || !forced_levels.empty();
   if (tit == tuned_.end())
     tit = tuned_.emplace(comp, std::vector<int>(maxL, (autotune && !forced) ? -1 : kIterDefaultVariant)).first;
+  auto in_part = [&](int l) { return !((part == 1 && l == 0) || (part == 2 && l > 0)); };
   bool need_tune = false;
-  for (int l = 0; l < maxL; l++)
-    if (!((part == 1 && l == 0) || (part == 2 && l > 0)) && tit->second[l] < 0) need_tune = true;
+  if (autotune && !forced) {
+    // a composition tuned before (by any engine of the process) is reused, so that every
+    // pair of a batch runs the same choice and only the first tunes
+    std::lock_guard<std::mutex> lk(shared_tuned_mutex());
+    auto& shared = shared_tuned();
+    auto sit = shared.find(comp);
+    for (int l = 0; l < maxL; l++) {
+      if (!in_part(l) || tit->second[l] >= 0) continue;
+      if (sit != shared.end() && l < (int)sit->second.size() && sit->second[l] >= 0) tit->second[l] = sit->second[l];
+      else need_tune = true;
+    }
+  }
   if (need_tune) {
     // first solve of this composition (and part): run it directly and tune while it runs
     std::vector<int> lv = tit->second;
     fused_solve_direct(pairs, masked, half, st, lv, true, concurrency, part);
     tit->second = lv;
+    {
+      std::lock_guard<std::mutex> lk(shared_tuned_mutex());
+      std::vector<int>& sv = shared_tuned()[comp];
+      sv.resize(maxL, -1);
+      for (int l = 0; l < maxL; l++)
+        if (in_part(l) && lv[l] >= 0) sv[l] = lv[l];
+    }
     note_variants(lv, part);
     return;
   }
