@@ -286,3 +286,23 @@ def test_fp16_batch_accuracy_at_full_size(gpu):
         d = np.abs(np.asarray(u, np.float64) - o.get("u"))[m]
         assert d.mean() <= 0.05, d.mean()
         assert (d > 1.0).mean() < 0.01
+
+
+def test_mask_change_between_frames_rebuilds_the_launches(gpu):
+    """A new mask between frames (graphs already captured under the old one) gives the same
+    bits as a handle that saw the same mask sequence on the drop-in path: the tile spans and
+    multi-iteration levels derived from the mask are not reused from stale graphs."""
+    w, h = 150, 110
+    i0, i1, mask, tv, cv = random_case(w, h, seed=1212)
+    yy, xx = np.mgrid[0:h, 0:w]
+    mask2 = ((xx - 40) ** 2 + (yy - 55) ** 2 < 45 ** 2).astype(np.float32)  # a different disc
+    p = params(n_levels=3, n_warp=2, n_iter=7)
+    ref = make(i0, i1, mask, tv, cv, p, fused=False)
+    f = make(i0, i1, mask, tv, cv, p, fused=True, half=False)
+    for frame in range(5):
+        if frame == 3:
+            ref.copyMaskToDevice(mask2)
+            f.copyMaskToDevice(mask2)
+        solve_frames(ref, i0, i1, True, 1)
+        solve_frames(f, i0, i1, True, 1)
+        assert np.array_equal(ref.debug_buffer("u", 1), f.debug_buffer("u", 1)), frame

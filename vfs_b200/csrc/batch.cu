@@ -513,6 +513,7 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
         }
       }
       s->codes_valid = true;
+      s->generation = next_generation();  // graphs captured under the old mask are not reused
     }
   }
 }

@@ -25,6 +25,11 @@ std::atomic<long long>& launch_counter() {
   return n;
 }
 
+uint64_t next_generation() {
+  static std::atomic<uint64_t> gen{0};
+  return ++gen;
+}
+
 std::atomic<bool>& pdl_enabled() {
   static std::atomic<bool> on{true};
   return on;
@@ -164,8 +169,7 @@ void StereoTgvImpl::initialize(const SolverParams& p) {
     throw ArgError{"initialize: invalid block or stride alignment"};
   release();
   if (!stream_) stream_ = own_stream();
-  static std::atomic<uint64_t> gen{0};
-  generation = ++gen;
+  generation = next_generation();
   P = p;
   width = p.width;
   height = p.height;

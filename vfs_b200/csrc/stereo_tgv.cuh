@@ -72,6 +72,9 @@ class FusedEngine {
   std::map<std::vector<int>, std::vector<int>> tuned_;
 };
 
+// process-wide counter of handle states (StereoTgvImpl::generation)
+uint64_t next_generation();
+
 // Device bytes a pair of this geometry allocates: the solver pool, and with `fused`
 // also the fused-path buffers.  Matches StereoTgvImpl::initialize / ensureFused.
 size_t estimate_device_bytes(int width, int height, int nLevels, float fScale, int strideAlignment, bool fused);
@@ -168,7 +171,9 @@ class StereoTgvImpl {
   // while a graph is captured, profiling events are created here (owned by the graph)
   std::vector<cudaEvent_t>* capture_events = nullptr;
   FusedEngine engine;  // single-pair fused solves
-  uint64_t generation = 0;  // incremented by every initialize (invalidates captured graphs)
+  // renewed by every initialize and every rebuild of the edge codes (a new mask): the tile
+  // spans and the multi-iteration levels baked into captured graphs follow the mask
+  uint64_t generation = 0;
 
  private:
   void release();
