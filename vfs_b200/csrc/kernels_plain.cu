@@ -32,6 +32,25 @@ __global__ void k_cv8u_to_gray(const uint8_t* src, float* dst, Geom g) {
   dst[idx] = (float)src[idx] / 256.0f;
 }
 
+// Both images of a pair from tight (row length w) u8 buffers into the pitched float planes,
+// with the same u8 / 256 conversion as k_cv8u_to_gray: a host upload is then one contiguous
+// copy per image.
+__global__ void k_cv8u_tight_to_gray2(const uint8_t* src0, const uint8_t* src1, float* dst0, float* dst1, Geom g) {
+  int ix, iy;
+  if (!pixel(ix, iy, g.w, g.h)) return;
+  const int si = ix + g.w * iy, di = ix + g.s * iy;
+  dst0[di] = (float)src0[si] / 256.0f;
+  dst1[di] = (float)src1[si] / 256.0f;
+}
+
+// A pitched plane of `comps` floats per pixel into a tight buffer (one contiguous download).
+__global__ void k_pack_tight(const float* src, float* dst, int comps, Geom g) {
+  int ix, iy;
+  if (!pixel(ix, iy, g.w, g.h)) return;
+  const long long si = ((long long)ix + (long long)g.s * iy) * comps, di = ((long long)ix + (long long)g.w * iy) * comps;
+  for (int c = 0; c < comps; c++) dst[di + c] = src[si + c];
+}
+
 __global__ void k_cv8uc3_to_gray(const uchar3* src, float* dst, Geom g) {
   int ix, iy;
   if (!pixel(ix, iy, g.w, g.h)) return;
@@ -462,6 +481,14 @@ __global__ void k_pack(const float* __restrict__ src, int comps, float* dst, Geo
 #define L2D(g) grid2d((g).w, (g).h), block2d(), 0, st
 void launch_cv8u_to_gray(const uint8_t* src, float* dst, Geom g, cudaStream_t st) {
   k_cv8u_to_gray<<<L2D(g)>>>(src, dst, g);
+  VFS_LAUNCH_CHECK();
+}
+void launch_cv8u_tight_to_gray2(const uint8_t* s0, const uint8_t* s1, float* d0, float* d1, Geom g, cudaStream_t st) {
+  k_cv8u_tight_to_gray2<<<L2D(g)>>>(s0, s1, d0, d1, g);
+  VFS_LAUNCH_CHECK();
+}
+void launch_pack_tight(const float* src, float* dst, int comps, Geom g, cudaStream_t st) {
+  k_pack_tight<<<L2D(g)>>>(src, dst, comps, g);
   VFS_LAUNCH_CHECK();
 }
 void launch_cv8uc3_to_gray(const uchar3* src, float* dst, Geom g, cudaStream_t st) {

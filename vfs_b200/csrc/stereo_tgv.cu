@@ -297,10 +297,12 @@ void StereoTgvImpl::copyImagesU8(const uint8_t* i0, const uint8_t* i1, bool devi
 void StereoTgvImpl::copyImagesU8On(const uint8_t* i0, const uint8_t* i1, cudaMemcpyKind kind, cudaStream_t st) {
   if (!initialized_) throw ArgError{"copyImagesToDevice before initialize"};
   if (!i0 || !i1) throw ArgError{"copyImagesToDevice: null image"};
-  VFS_CUDA(cudaMemcpy2DAsync(d_i08u, stride, i0, width, width, height, kind, st));
-  VFS_CUDA(cudaMemcpy2DAsync(d_i18u, stride, i1, width, width, height, kind, st));
-  launch_cv8u_to_gray(d_i08u, pI0[0], geom(0), st);
-  launch_cv8u_to_gray(d_i18u, pI1[0], geom(0), st);
+  // one contiguous copy per image into the staging buffers (tight rows), then one kernel
+  // converts both into the pitched planes
+  const size_t n = (size_t)width * height;
+  VFS_CUDA(cudaMemcpyAsync(d_i08u, i0, n, kind, st));
+  VFS_CUDA(cudaMemcpyAsync(d_i18u, i1, n, kind, st));
+  launch_cv8u_tight_to_gray2(d_i08u, d_i18u, pI0[0], pI1[0], geom(0), st);
 }
 
 void StereoTgvImpl::copyImagesF32(const float* i0, const float* i1) {
@@ -464,6 +466,12 @@ void StereoTgvImpl::copyOutOn(const char* what, float* dst, cudaMemcpyKind kind,
   else if (!std::strcmp(what, "X")) { src = d_X; comps = 3; }
   else if (!std::strcmp(what, "rgb")) { src = d_uvrgb; comps = 3; }
   else throw ArgError{std::string("copy: unknown buffer ") + what};
+  if (kind == cudaMemcpyDeviceToHost) {
+    // pack on the device, then one contiguous download
+    launch_pack_tight((const float*)src, d_pack, comps, geom(0), st);
+    VFS_CUDA(cudaMemcpyAsync(dst, d_pack, (size_t)width * height * comps * sizeof(float), kind, st));
+    return;
+  }
   size_t row = (size_t)width * comps * sizeof(float);
   VFS_CUDA(cudaMemcpy2DAsync(dst, row, src, (size_t)stride * comps * sizeof(float), row, height, kind, st));
 }
