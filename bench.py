@@ -325,11 +325,8 @@ def run_ours(args, rank, world, local):
 
     def device_step():
         if fused:
-            for s, (a, b) in zip(solvers, d_imgs):
-                s.copy_images_from_device(a, b)
-            sbatch.solve(True)
-            for s, o in zip(solvers, d_out):
-                s.copy_1d_disparity_to_device(o)
+            # one call: per pair (on its own lane) the device copy in, solve, copy out
+            sbatch.solve_device(d_imgs, d_out)
             return
         for s, (a, b), o in zip(solvers, d_imgs, d_out):
             s.copy_images_from_device(a, b)

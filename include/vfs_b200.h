@@ -149,6 +149,11 @@ int vfs_batch_solve(vfs_batch* b, int masked);
  * engines; pageable ones work but are staged by the driver. */
 int vfs_batch_solve_host(vfs_batch* b, const uint8_t* const* i0, const uint8_t* const* i1,
                          float* const* u_out, int masked);
+/* The same with the images and disparities in device memory (e.g. frames decoded on the GPU):
+ * tight W x H u8 inputs and W x H float32 outputs.  Stream-ordered on the batch's stream:
+ * returns after enqueueing. */
+int vfs_batch_solve_device(vfs_batch* b, const uint8_t* const* d_i0, const uint8_t* const* d_i1,
+                           float* const* d_u_out, int masked);
 /* The fused path picks the tile height of its iteration kernel per pyramid level by timing
  * the variants on the first solve of each batch composition (on by default); the timing
  * launches do not change results.  Off: the default 31 x 8 tiles everywhere. */

@@ -306,3 +306,30 @@ def test_mask_change_between_frames_rebuilds_the_launches(gpu):
         solve_frames(ref, i0, i1, True, 1)
         solve_frames(f, i0, i1, True, 1)
         assert np.array_equal(ref.debug_buffer("u", 1), f.debug_buffer("u", 1)), frame
+
+
+def test_batch_solve_device_matches_host_buffers(gpu):
+    """vfs_batch_solve_device (images and disparities in device memory, copies on each pair's
+    lane) gives the bits of vfs_batch_solve_host, over two frames, split schedule included."""
+    import torch
+    from vfs_b200.stereotgv import StereoBatch
+    cases = [(96, 64, 2), (130, 101, 3), (67, 53, 2)]
+    p0 = params(n_warp=2, n_iter=6)
+    hb, db = StereoBatch(half_storage=True), StereoBatch(half_storage=True)
+    db.set_fine_concurrency(1)
+    data = []
+    for k, (w, h, L) in enumerate(cases):
+        i0, i1, mask, tv, cv = random_case(w, h, seed=1400 + k)
+        p = dict(p0, n_levels=L)
+        hb.add(make(i0, i1, mask, tv, cv, p, fused=True, half=True))
+        db.add(make(i0, i1, mask, tv, cv, p, fused=True, half=True))
+        data.append((i0, i1))
+    d_in = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b in data]
+    d_out = [torch.full((h, w), -1.0, device="cuda") for (w, h, _) in cases]
+    torch.cuda.synchronize()  # the batch's streams do not wait for the default stream
+    for frame in range(2):
+        want = hb.solve_host(data)
+        db.solve_device(d_in, d_out)
+        torch.cuda.synchronize()
+        for k, (g, w_) in enumerate(zip(d_out, want)):
+            assert np.array_equal(g.cpu().numpy(), w_), (frame, k)

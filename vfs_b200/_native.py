@@ -74,6 +74,7 @@ SIGNATURES = {
     "vfs_batch_set_graph": [_vp, _i],
     "vfs_batch_solve": [_vp, _i],
     "vfs_batch_solve_host": [_vp, _vp, _vp, _vp, _i],
+    "vfs_batch_solve_device": [_vp, _vp, _vp, _vp, _i],
     "vfs_batch_set_autotune": [_vp, _i],
     "vfs_batch_set_mode": [_vp, _i],
     "vfs_batch_set_fine_concurrency": [_vp, _i],

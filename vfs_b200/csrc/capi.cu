@@ -424,6 +424,7 @@ struct BatchHostIO {
   const uint8_t* const* i0 = nullptr;
   const uint8_t* const* i1 = nullptr;
   float* const* u = nullptr;
+  bool device = false;  // the buffers are in device memory (copies stay on the device)
 };
 
 void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
@@ -446,10 +447,11 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
   if (b->mode == VFS_BATCH_ONE_LAUNCH) {
     if (io)
       for (size_t k = 0; k < pairs.size(); k++)
-        pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], cudaMemcpyHostToDevice, b->stream);
+        pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], io->device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->stream);
     b->engine.solve(pairs, masked != 0, b->half, b->stream);
     if (io)
-      for (size_t k = 0; k < pairs.size(); k++) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, b->stream);
+      for (size_t k = 0; k < pairs.size(); k++)
+        pairs[k]->copyOutOn("u", io->u[k], io->device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->stream);
   } else {
     // fork: every pair's upload, solve (its own graph) and download on its own slot
     // stream, then join; one pair's copies overlap the other pairs' solves
@@ -531,13 +533,16 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
       // parts follow there), so that full-resolution work starts early
       cudaStream_t cl = (split && b->fine_priority >= 2 && k < S) ? b->fine_lanes[k] : b->lanes[k];
       if (cl != b->lanes[k]) VFS_CUDA(cudaStreamWaitEvent(cl, b->start, 0));
-      if (io) pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], cudaMemcpyHostToDevice, cl);
+      if (io)
+        pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], io->device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                 cl);
       run(k, split ? 1 : 0, n, cl, cl != b->lanes[k]);
       if (split) {
         VFS_CUDA(cudaEventRecord(b->coarse_done[k], cl));
         continue;
       }
-      if (io) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, b->lanes[k]);
+      if (io)
+        pairs[k]->copyOutOn("u", io->u[k], io->device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->lanes[k]);
       VFS_CUDA(cudaEventRecord(b->lane_done[k], b->lanes[k]));
       VFS_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
     }
@@ -548,7 +553,7 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
         if (k >= S) VFS_CUDA(cudaStreamWaitEvent(fl, b->fine_done[k - S], 0));
         run(k, 2, S, fl, b->fine_priority >= 1);
         VFS_CUDA(cudaEventRecord(b->fine_done[k], fl));
-        if (io) pairs[k]->copyOutOn("u", io->u[k], cudaMemcpyDeviceToHost, fl);
+        if (io) pairs[k]->copyOutOn("u", io->u[k], io->device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, fl);
         VFS_CUDA(cudaEventRecord(b->lane_done[k], fl));
         VFS_CUDA(cudaStreamWaitEvent(b->stream, b->lane_done[k], 0));
         // the next solve's parts of this slot follow this one's end
@@ -560,7 +565,7 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
   VFS_CUDA(cudaEventRecord(b->done, b->stream));
   for (auto* p : pairs)
     if (p->stream() != b->stream) VFS_CUDA(cudaStreamWaitEvent(p->stream(), b->done, 0));
-  if (io) VFS_CUDA(cudaStreamSynchronize(b->stream));
+  if (io && !io->device) VFS_CUDA(cudaStreamSynchronize(b->stream));
 }
 
 }  // namespace
@@ -575,7 +580,16 @@ int vfs_batch_solve_host(vfs_batch* b, const uint8_t* const* i0, const uint8_t* 
                          int masked) {
   return guarded(b, [&] {
     if (!i0 || !i1 || !u_out) throw vfs::ArgError{"batch solve: null host buffer list"};
-    BatchHostIO io{i0, i1, u_out};
+    BatchHostIO io{i0, i1, u_out, false};
+    batch_solve(b, masked, &io);
+  });
+}
+
+int vfs_batch_solve_device(vfs_batch* b, const uint8_t* const* d_i0, const uint8_t* const* d_i1, float* const* d_u_out,
+                           int masked) {
+  return guarded(b, [&] {
+    if (!d_i0 || !d_i1 || !d_u_out) throw vfs::ArgError{"batch solve: null device buffer list"};
+    BatchHostIO io{d_i0, d_i1, d_u_out, true};
     batch_solve(b, masked, &io);
   });
 }

@@ -66,6 +66,7 @@ class _Lane:
     batch: StereoBatch
     event: object = None
     requests: List[Request] = field(default_factory=list)
+    ins: list = field(default_factory=list)
     outs: list = field(default_factory=list)
     hosts: list = field(default_factory=list)
 
@@ -166,7 +167,7 @@ class StereoServer:
                     cam.frames += 1
                     fin.append(r)
                 lane.event = None
-                lane.requests, lane.outs, lane.hosts = [], [], []
+                lane.requests, lane.ins, lane.outs, lane.hosts = [], [], [], []
         self.done.extend(fin)
         return fin
 
@@ -190,28 +191,32 @@ class StereoServer:
         lane.batch.clear()
         now = time.perf_counter()
         with torch.cuda.stream(st):
+            ins, outs = [], []
             for r in picked:
                 cam = self.cameras[r.stream_id]
                 cam.busy = True
                 cam.solver.set_stream(st)
                 a = torch.from_numpy(np.ascontiguousarray(r.i0)).pin_memory().to(self.device, non_blocking=True)
                 b = torch.from_numpy(np.ascontiguousarray(r.i1)).pin_memory().to(self.device, non_blocking=True)
-                cam.solver.copy_images_from_device(a, b)
+                ins.append((a, b))
+                outs.append(torch.empty((cam.height, cam.width), dtype=torch.float32, device=self.device))
                 if self.path != "plain":
                     lane.batch.add(cam.solver)
                 r.t_launch = now
             if self.path == "plain":
-                self.cameras[picked[0].stream_id].solver.solveStereoForwardMasked()
+                solver = self.cameras[picked[0].stream_id].solver
+                solver.copy_images_from_device(*ins[0])
+                solver.solveStereoForwardMasked()
+                solver.copy_1d_disparity_to_device(outs[0])
             else:
-                lane.batch.solve(True)
-            for r in picked:
-                cam = self.cameras[r.stream_id]
-                out = torch.empty((cam.height, cam.width), dtype=torch.float32, device=self.device)
-                cam.solver.copy_1d_disparity_to_device(out)
+                # each request's copies and solve on its own lane of the batch
+                lane.batch.solve_device(ins, outs)
+            for out in outs:
                 host = torch.empty(out.shape, dtype=torch.float32, pin_memory=True)
                 host.copy_(out, non_blocking=True)
                 lane.outs.append(out)
                 lane.hosts.append(host)
+            lane.ins = ins  # kept alive until the batch completes
             ev = torch.cuda.Event()
             ev.record(st)
         lane.event = ev

@@ -338,6 +338,23 @@ class StereoBatch:
     def solve(self, masked: bool = True) -> None:
         check_batch(self._h, self._L.vfs_batch_solve(self._h, int(masked)))
 
+    def solve_device(self, images, outputs, masked: bool = True) -> None:
+        """One solve of every pair from and to device memory: ``images[k] = (i0, i1)``, tight
+        H x W uint8 CUDA tensors of pair k, and ``outputs[k]`` H x W float32 CUDA tensors.
+        Stream-ordered on the batch's stream."""
+        n = len(self.members)
+        if len(images) != n or len(outputs) != n:
+            raise VfsError(-1, f"solve_device: {len(images)} image pairs and {len(outputs)} outputs for a batch of {n}")
+        for m, (a, b), o in zip(self.members, images, outputs):
+            for t in (a, b, o):
+                if not (t.is_cuda and t.is_contiguous() and tuple(t.shape) == (m.height, m.width)):
+                    raise VfsError(-1, "solve_device: need contiguous H x W CUDA tensors")
+        P = ctypes.c_void_p * n
+        i0 = P(*[a.data_ptr() for a, _ in images])
+        i1 = P(*[b.data_ptr() for _, b in images])
+        uo = P(*[o.data_ptr() for o in outputs])
+        check_batch(self._h, self._L.vfs_batch_solve_device(self._h, i0, i1, uo, int(masked)))
+
     def solve_host(self, images, outputs=None, masked: bool = True):
         """One solve of every pair from and to host memory: ``images[k] = (i0, i1)``, tight
         H x W uint8 arrays of pair k; the disparities go to ``outputs[k]`` (H x W float32,
