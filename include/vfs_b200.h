@@ -146,7 +146,7 @@ int vfs_batch_solve(vfs_batch* b, int masked);
  * disparity to u_out[k].  Each pair's upload, solve and download are queued on that pair's
  * lane, so the copies of one pair overlap the solves of the others.  Returns when every
  * output is in host memory.  Page-locked host buffers are copied asynchronously by the copy
- * engines; pageable ones work but are staged by the driver. */
+ * engines; pageable ones work but are staged by the CUDA driver. */
 int vfs_batch_solve_host(vfs_batch* b, const uint8_t* const* i0, const uint8_t* const* i1,
                          float* const* u_out, int masked);
 /* The same with the images and disparities in device memory (e.g. frames decoded on the GPU):

@@ -1,7 +1,7 @@
 """ctypes wrapper of the CPU oracle (oracle/tgv_oracle.cpp).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()`` (as the
-checker) and by ``bench.py``'s CPU-baseline leg.  The product package ``vfs_b200``
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()`` (to check the
+CUDA result) and by ``bench.py``'s CPU-baseline leg.  The product package ``vfs_b200``
 never imports it.
 
 The class mirrors the reference ``StereoTgv`` host API (stereotgv/stereotgv.h:107-124):

@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter_x2(const __g
   griddep_wait();  // the previous iteration's outputs are this one's inputs
   griddep_launch_dependents();
 
-  // ---- round 1: edge codes and tensor ----------------------------------------------------
+  // ---- first load round: edge codes and tensor ----------------------------------------------
   uint8_t cA, cB;
   float aA, aB, bA, bB, ccA, ccB;
   ld_pair(P.code, pos, inA, inB, (uint8_t)0, cA, cB);
@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter_x2(const __g
   // another block needs, so it leaves here
   if (MASKED && !__syncthreads_or((inA && (cA & kOn)) || (inB && (cB & kOn)))) return;
 
-  // ---- round 2 ---------------------------------------------------------------------------
+  // ---- second load round --------------------------------------------------------------------
   // the dual step runs at A for lanes >= 1 (region column >= 2) and at B for every lane
   const bool dA = inA && L >= 1, dB = inB;
   const bool fullA = dA && (cA & kOn), fullB = dB && (cB & kOn);  // the full dual update
