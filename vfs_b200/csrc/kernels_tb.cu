@@ -27,6 +27,7 @@
 #include "tgv_pixel.cuh"
 #include "tgv_pixel_fast.cuh"
 
+#include <atomic>
 #include <type_traits>
 
 namespace vfs {
@@ -34,6 +35,7 @@ namespace vfs {
 namespace {
 
 constexpr int kTBX = 32;  // threads of a block in x (its y extent BY is a template parameter)
+constexpr int kMaxDevices = 64;
 
 template <class ST, int K, int TX, int TY>
 struct TBLayout {
@@ -297,10 +299,13 @@ template <bool MASKED, class ST, int K, int TX, int TY, int BY>
 void launch_tb_k(const IterTBArgs& A, cudaStream_t st) {
   typedef TBLayout<ST, K, TX, TY> L;
   auto k = k_fused_iter_tb<MASKED, ST, K, TX, TY, BY>;
-  static bool configured = false;  // per instantiation
-  if (!configured) {
+  // the shared-memory limit is raised once per instantiation and device
+  static std::atomic<bool> configured[kMaxDevices];
+  int dev = 0;
+  VFS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices || !configured[dev].load(std::memory_order_acquire)) {
     VFS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::kBytes));
-    configured = true;
+    if (dev >= 0 && dev < kMaxDevices) configured[dev].store(true, std::memory_order_release);
   }
   const dim3 grid((A.P.w + TX - 1) / TX, (A.P.h + TY - 1) / TY), blk(kTBX, BY);
   launch_overlapped_smem(k, grid, blk, L::kBytes, st, A);
