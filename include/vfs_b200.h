@@ -187,11 +187,12 @@ int vfs_set_autotune(vfs_stereo* s, int on);
  * neighbours' T p and q through shared memory; 3-5: one warp per 31-column strip of 8, 16
  * or 32 rows, neighbours by warp shuffle and registers; 6-9: several iterations per launch
  * with the tile's region held in shared memory (6: 3 iterations on 64 x 24 tiles, 7: 5 on
- * 32 x 24, 8: 3 on 23 x 23, 9: 5 on 17 x 17); 10-11: two horizontally adjacent pixels per
- * thread on 62 x 8 / 62 x 4 tiles.  6-11 apply to one-pair launches (other launches, and
- * levels where they do not apply, use variant 1).  Every variant gives the same results;
- * this selects speed only.  (No counterpart in the reference.) */
-#define VFS_ITER_VARIANTS 12
+ * 32 x 24, 8: 3 on 23 x 23, 9: 5 on 17 x 17, 12: 7 on 11 x 11, 13: 9 on 5 x 5); 10-11: two
+ * horizontally adjacent pixels per thread on 62 x 8 / 62 x 4 tiles.  6-13 apply to one-pair
+ * launches (other launches, and levels where they do not apply, use variant 1).  Every
+ * variant gives the same results; this selects speed only.  (No counterpart in the
+ * reference.) */
+#define VFS_ITER_VARIANTS 14
 int vfs_set_iteration_variant(vfs_stereo* s, int variant);
 /* Force one variant per pyramid level (finest first; levels beyond n_levels use variant 1),
  * e.g. to pin a tuned choice; n_levels = 0 clears it. */

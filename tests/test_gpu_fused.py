@@ -146,14 +146,15 @@ def test_batch_solve_host_matches_device_path(gpu, one_launch):
 @pytest.mark.parametrize("masked", [True, False])
 def test_every_iteration_variant_bit_identical(gpu, masked):
     """All variants of the fused iteration kernel (shared-memory tiles of 4 / 8 / 16 rows,
-    row-streaming strips of 8 / 16 / 32 rows, 3 or 5 iterations per launch on tiles held in
-    shared memory, two pixels per thread on 62-column tiles) give the drop-in path's bits with float storage and one another's bits
-    with half storage, on sizes that cut tiles unevenly.  7 iterations per warp leave a
-    remainder after the multi-iteration launches.  The 64 x 48 case has no row padding at
+    row-streaming strips of 8 / 16 / 32 rows, 3 to 9 iterations per launch on tiles held in
+    shared memory, two pixels per thread on 62-column tiles) give the drop-in path's bits
+    with float storage and one another's bits with half storage, on sizes that cut tiles
+    unevenly.  11 iterations per warp leave a remainder after the multi-iteration launches
+    of every K (3, 5, 7, 9).  The 64 x 48 case has no row padding at
     level 0 and an all-on mask, where the multi-iteration kernel must fall back."""
     from vfs_b200.stereotgv import StereoBatch
     cases = [(97, 71, 2), (131, 45, 3), (40, 100, 2), (64, 48, 2)]
-    p0 = params(n_warp=2, n_iter=7)
+    p0 = params(n_warp=2, n_iter=11)
     for k, (w, h, L) in enumerate(cases):
         i0, i1, mask, tv, cv = random_case(w, h, seed=500 + k, circle=(w, h) != (64, 48))
         p = dict(p0, n_levels=L)
@@ -161,7 +162,7 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
         solve_frames(ref, i0, i1, masked, 2)
         want = {n: ref.debug_buffer(n, c) for n, c in (("u", 1), ("u_", 1), ("warpUV", 2), ("Tp", 2))}
         half_ref = None
-        for variant in range(12):
+        for variant in range(14):
             s = make(i0, i1, mask, tv, cv, p, fused=True)
             s.set_iteration_variant(variant)
             solve_frames(s, i0, i1, masked, 2)
@@ -216,22 +217,23 @@ def test_launch_overlap_does_not_change_results(gpu):
 
 
 def test_per_level_variants_and_tuned_choice_reported(gpu):
-    """A per-level variant list (here one-iteration at full resolution, five iterations per
-    launch below) gives the drop-in path's bits, and the handle reports what it ran."""
+    """A per-level variant list (here one-iteration at full resolution, nine and seven
+    iterations per launch below) gives the drop-in path's bits, and the handle reports what
+    it ran; the tuner never picks a row-streaming variant."""
     i0, i1, mask, tv, cv = random_case(120, 90, seed=808)
     p = params(n_levels=3, n_warp=2, n_iter=11)
     ref = make(i0, i1, mask, tv, cv, p, fused=False)
     solve_frames(ref, i0, i1, True, 2)
     s = make(i0, i1, mask, tv, cv, p, fused=True)
-    s.set_iteration_variants([1, 9, 8])
+    s.set_iteration_variants([1, 13, 12])  # 9 and 7 iterations per launch, remainders single
     solve_frames(s, i0, i1, True, 2)
-    assert s.iteration_variants() == [1, 9, 8]
+    assert s.iteration_variants() == [1, 13, 12]
     for n, c in (("u", 1), ("warpUV", 2), ("Tp", 2)):
         assert np.array_equal(s.debug_buffer(n, c), ref.debug_buffer(n, c)), n
     t = make(i0, i1, mask, tv, cv, p, fused=True)
     solve_frames(t, i0, i1, True, 1)  # autotuned
     v = t.iteration_variants()
-    assert len(v) == 3 and all(0 <= x < 10 for x in v)
+    assert len(v) == 3 and all(0 <= x < 14 and not 3 <= x <= 5 for x in v)
 
 
 @pytest.mark.parametrize("fine,stagger,prio", [(1, 0, 0), (2, 0, 2), (2, 1, 1), (3, 1, 0)])

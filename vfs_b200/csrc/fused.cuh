@@ -125,7 +125,7 @@ void launch_fused_iteration_rows(const IterArgs& A, bool masked, bool half_stora
                                  int rows);
 
 // ---- K consecutive primal-dual iterations of one pair in one launch (kernels_tb.cu) ----
-constexpr int kIterTBMax = 5;
+constexpr int kIterTBMax = 9;
 struct IterTBArgs {
   IterPair P;  // pointers of the launch's first iteration (its outputs: us, u_s, v_s)
   float sp[kIterTBMax], sq[kIterTBMax], tau[kIterTBMax], mu[kIterTBMax];  // per iteration
@@ -256,14 +256,17 @@ inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFT
 // 5 on 32 x 24, and with one region pixel per thread 3 on 23 x 23 and 5 on 17 x 17 tiles.
 // variants 10-11: k_fused_iter_x2, two horizontally adjacent pixels per thread on 62 x 8 /
 // 62 x 4 tiles (kernels_x2.cu); one pair per launch only.
-constexpr int kIterVariants = 12;
-constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17, 8, 4};
-constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 3, 6};
+// variants 12-13: k_fused_iter_tb with one region pixel per thread, 7 iterations on 11 x 11
+// tiles and 9 on 5 x 5 tiles (for the smallest levels, where the GPU is mostly idle).
+constexpr int kIterVariants = 14;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17, 8, 4, 11, 5};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 3, 6, 0, 0};
 constexpr int kIterFirstRowsVariant = 3;
 constexpr int kIterFirstTBVariant = 6;
 constexpr int kIterFirstX2Variant = 10;
 // variants whose launch carries one pair only (others fall back to the default there)
 inline bool iter_variant_single_pair(int v) { return v >= kIterFirstTBVariant; }
+constexpr int kIterFirstDeepTBVariant = 12;
 constexpr int kIterDefaultVariant = 1;
 inline int iter_tiles_x_of(int w) { return (w + 30) / 31; }
 inline int iter_tiles_of(int w, int h, int rows) { return iter_tiles_x_of(w) * ((h + rows - 1) / rows); }

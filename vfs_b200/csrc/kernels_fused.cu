@@ -281,7 +281,7 @@ double iteration_gpu_share(int variant, bool masked, bool half, int w, int h) {
   // blocks of the launch and resident blocks per SM of the variant's kernel (one pair)
   long long blocks = 0;
   int per_sm = 0;
-  if (variant >= kIterFirstX2Variant) {
+  if (variant >= kIterFirstX2Variant && variant < kIterFirstDeepTBVariant) {
     return x2_gpu_share(variant, masked, half, w, h);
   } else if (variant >= kIterFirstTBVariant) {
     return tb_gpu_share(variant, masked, half, w, h);
@@ -311,7 +311,7 @@ void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, c
     launch_fused_iteration_rows(A, masked, half_storage, st, parity, kIterVariantRows[variant]);
     return;
   }
-  if (variant >= kIterFirstX2Variant && variant < kIterVariants) {
+  if (variant >= kIterFirstX2Variant && variant < kIterFirstDeepTBVariant) {
     launch_fused_iteration_x2(A, masked, half_storage, st, parity, variant);
     return;
   }

@@ -353,6 +353,8 @@ int tb_iterations(int variant) {
     case kIterFirstTBVariant + 1: return 5;
     case kIterFirstTBVariant + 2: return 3;
     case kIterFirstTBVariant + 3: return 5;
+    case kIterFirstDeepTBVariant: return 7;
+    case kIterFirstDeepTBVariant + 1: return 9;
     default: return 1;
   }
 }
@@ -363,6 +365,8 @@ double tb_gpu_share(int variant, bool masked, bool half, int w, int h) {
     case kIterFirstTBVariant + 1: return tb_share<5, 32, 24, 16>(masked, half, w, h);
     case kIterFirstTBVariant + 2: return tb_share<3, 23, 23, 32>(masked, half, w, h);
     case kIterFirstTBVariant + 3: return tb_share<5, 17, 17, 32>(masked, half, w, h);
+    case kIterFirstDeepTBVariant: return tb_share<7, 11, 11, 32>(masked, half, w, h);
+    case kIterFirstDeepTBVariant + 1: return tb_share<9, 5, 5, 32>(masked, half, w, h);
     default: throw ArgError{"not a temporally blocked iteration variant"};
   }
 }
@@ -375,6 +379,8 @@ void launch_fused_iteration_tb(const IterTBArgs& A, bool masked, bool half_stora
     // one region pixel per thread: 32 x 32 regions
     case kIterFirstTBVariant + 2: launch_tb_3<3, 23, 23, 32>(A, masked, half_storage, st); break;
     case kIterFirstTBVariant + 3: launch_tb_3<5, 17, 17, 32>(A, masked, half_storage, st); break;
+    case kIterFirstDeepTBVariant: launch_tb_3<7, 11, 11, 32>(A, masked, half_storage, st); break;
+    case kIterFirstDeepTBVariant + 1: launch_tb_3<9, 5, 5, 32>(A, masked, half_storage, st); break;
     default: throw ArgError{"not a temporally blocked iteration variant"};
   }
   VFS_LAUNCH_CHECK();
