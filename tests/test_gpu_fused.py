@@ -147,7 +147,8 @@ def test_batch_solve_host_matches_device_path(gpu, one_launch):
 def test_every_iteration_variant_bit_identical(gpu, masked):
     """All variants of the fused iteration kernel (shared-memory tiles of 4 / 8 / 16 rows,
     row-streaming strips of 8 / 16 / 32 rows, 3 to 9 iterations per launch on tiles held in
-    shared memory, two pixels per thread on 62-column tiles) give the drop-in path's bits
+    shared memory, two pixels per thread on 62-column tiles, the whole level in the shared
+    memory of a 16- or 8-CTA cluster) give the drop-in path's bits
     with float storage and one another's bits with half storage, on sizes that cut tiles
     unevenly.  11 iterations per warp leave a remainder after the multi-iteration launches
     of every K (3, 5, 7, 9).  The 64 x 48 case has no row padding at
@@ -162,7 +163,7 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
         solve_frames(ref, i0, i1, masked, 2)
         want = {n: ref.debug_buffer(n, c) for n, c in (("u", 1), ("u_", 1), ("warpUV", 2), ("Tp", 2))}
         half_ref = None
-        for variant in range(14):
+        for variant in range(16):
             s = make(i0, i1, mask, tv, cv, p, fused=True)
             s.set_iteration_variant(variant)
             solve_frames(s, i0, i1, masked, 2)
@@ -195,6 +196,36 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
         solve_frames(s, i0, i1, masked, 1)
         m.synchronize()
         assert np.array_equal(s.debug_buffer("u", 1), m.debug_buffer("u", 1))
+
+
+@pytest.mark.parametrize("masked", [True, False])
+@pytest.mark.parametrize("n_iter", [10, 67])
+def test_cluster_resident_iteration_counts(gpu, masked, n_iter):
+    """The cluster-resident variants (14: 16 CTAs, 15: 8 CTAs) with an even number of
+    iterations per warp (the results stay in the launch's input buffers) and with more
+    iterations than one launch takes (64 + 3), over two frames and with CUDA graphs: the
+    drop-in path's bits with float storage, variant 1's bits with half storage.  Heights of
+    45 and 22 rows leave trailing CTAs without rows; 200 x 90 with 8 CTAs gives each thread
+    three pixels."""
+    for (w, h, L) in [(97, 71, 2), (131, 45, 2), (200, 90, 2)]:
+        i0, i1, mask, tv, cv = random_case(w, h, seed=w * h + n_iter)
+        p = params(n_levels=L, n_warp=2, n_iter=n_iter)
+        ref = make(i0, i1, mask, tv, cv, p, fused=False)
+        solve_frames(ref, i0, i1, masked, 2)
+        href = make(i0, i1, mask, tv, cv, p, fused=True, half=True)
+        href.set_iteration_variant(1)
+        solve_frames(href, i0, i1, masked, 2)
+        hu = href.copy1DDisparityToHost()
+        for variant in (14, 15):
+            s = make(i0, i1, mask, tv, cv, p, fused=True)
+            s.set_iteration_variant(variant)
+            solve_frames(s, i0, i1, masked, 2)
+            for n, c in (("u", 1), ("u_", 1), ("warpUV", 2), ("Tp", 2)):
+                assert np.array_equal(s.debug_buffer(n, c), ref.debug_buffer(n, c)), (w, h, variant, n)
+            sh = make(i0, i1, mask, tv, cv, p, fused=True, half=True)
+            sh.set_iteration_variant(variant)
+            solve_frames(sh, i0, i1, masked, 2)
+            assert np.array_equal(sh.copy1DDisparityToHost(), hu), (w, h, variant, "half")
 
 
 def test_launch_overlap_does_not_change_results(gpu):
@@ -233,7 +264,7 @@ def test_per_level_variants_and_tuned_choice_reported(gpu):
     t = make(i0, i1, mask, tv, cv, p, fused=True)
     solve_frames(t, i0, i1, True, 1)  # autotuned
     v = t.iteration_variants()
-    assert len(v) == 3 and all(0 <= x < 14 and not 3 <= x <= 5 for x in v)
+    assert len(v) == 3 and all(0 <= x < 16 and not 3 <= x <= 5 for x in v)
 
 
 @pytest.mark.parametrize("fine,stagger,prio", [(1, 0, 0), (2, 0, 2), (2, 1, 1), (3, 1, 0)])

@@ -245,6 +245,28 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         T.write_tp = 0;
         return T;
       };
+      // the cluster-resident kernel: the same schedule for k (up to kCLMaxIters) iterations
+      auto cl_args = [&](int variant_, float sigma_, float tau_, int iter0, int k) {
+        IterCLArgs C{};
+        C.P = iter_args(kIterDefaultVariant, sigma_, tau_, 1.0f, 0).pr[0];
+        for (int j = 0; j < k; j++) {
+          float mu_;
+          if (sigma_ < 1000.0f) mu_ = 1.0f / std::sqrt(1 + 0.7f * tau_ * P0.timestep_lambda);
+          else mu_ = 1;
+          C.sp[j] = act[0]->P.alpha1 * sigma_ / 3.0f;
+          C.sq[j] = act[0]->P.alpha0 * sigma_ / 2.0f;
+          C.tau[j] = tau_;
+          C.mu[j] = mu_;
+          sigma_ = sigma_ / mu_;
+          tau_ = tau_ * mu_;
+        }
+        C.n = k;
+        C.parity = iter0 & 1;
+        C.write_tp = 0;
+        C.rows = cluster_rows(variant_, C.P.h);
+        return C;
+      };
+      const int lw = act[0]->pW[level], lh = act[0]->pH[level];
       if (level_variant[level] < 0) {
         if (can_tune && warpIter == 0 && P0.nSolverIters > 0) {
           // Time every tile variant on this level's data.  These launches read the same
@@ -269,10 +291,18 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             const int kv = tb_iterations(v);
             if (kv > 1 && (!tb_here || kv > P0.nSolverIters)) continue;
             if (iter_variant_single_pair(v) && na != 1) continue;
-            IterArgs T = iter_args(kv > 1 ? kIterDefaultVariant : v, 1.0f, 1.0f, mu0, 0);
+            const bool clv = iter_variant_cluster(v);
+            if (clv && (!tb_here || !cluster_fits(v, masked, half, lw, lh))) continue;
+            // the cluster-resident kernel is timed over an odd number of iterations, so that it
+            // writes the other ping-pong buffers, which the first iteration below overwrites
+            const int kc = clv ? ((std::min(P0.nSolverIters, kCLMaxIters) - 1) | 1) : 1;
+            IterArgs T = iter_args((kv > 1 || clv) ? kIterDefaultVariant : v, 1.0f, 1.0f, mu0, 0);
             IterTBArgs TB = tb_args(1.0f, 1.0f, 0, kv);
+            IterCLArgs CL{};
+            if (clv) CL = cl_args(v, 1.0f, 1.0f, 0, kc);
             auto once = [&] {
-              if (kv > 1) launch_fused_iteration_tb(TB, masked, half, st, v);
+              if (clv) launch_fused_iteration_cluster(CL, masked, half, st, v);
+              else if (kv > 1) launch_fused_iteration_tb(TB, masked, half, st, v);
               else launch_fused_iteration(T, masked, half, st, 0, v);
             };
             once();  // warm the caches / the instruction path
@@ -282,12 +312,12 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             VFS_CUDA(cudaEventSynchronize(e1));
             float ms = 0;
             VFS_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-            ms /= (float)kv;  // per iteration
+            ms /= (float)(clv ? kc : kv);  // per iteration
             best_ms[v] = std::min(best_ms[v], ms);
             if (pass == 0) continue;
             ms = best_ms[v];
             double share = 1.0;
-            if (na == 1) share = iteration_gpu_share(v, masked, half, act[0]->pW[level], act[0]->pH[level]);
+            if (na == 1) share = iteration_gpu_share(v, masked, half, lw, lh);
             double cost = (double)ms * std::max(share, floor_share);
             // the default keeps its place unless another variant is clearly (5 %) cheaper
             if (v == kIterDefaultVariant) cost *= 0.95;
@@ -306,17 +336,29 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
       const int variant = level_variant[level] < 0 ? kIterDefaultVariant : level_variant[level];
       // K iterations per launch where the variant is a multi-iteration one and it applies
       // here; the remaining iterations (and the fallback) use the default one-iteration form
-      const int K = tb_here ? tb_iterations(variant) : 1;
-      const int v1 = (tb_iterations(variant) > 1 || (iter_variant_single_pair(variant) && na != 1))
+      // (the cluster-resident kernel: all iterations, in launches of up to kCLMaxIters)
+      const bool cl_here = tb_here && iter_variant_cluster(variant) && cluster_fits(variant, masked, half, lw, lh);
+      const int K = cl_here ? kCLMaxIters : tb_here ? tb_iterations(variant) : 1;
+      const int v1 = (tb_iterations(variant) > 1 || iter_variant_cluster(variant) ||
+                      (iter_variant_single_pair(variant) && na != 1))
                          ? kIterDefaultVariant
                          : variant;
       float tau = 1.0f;
       float sigma = 1.0f / tau;
       const int n_it = P0.nSolverIters;
-      prof->profBeginPx(kProfFused, px_level, n_it, st, K > 1 ? n_it / K + n_it % K : n_it);
+      prof->profBeginPx(kProfFused, px_level, n_it, st,
+                        cl_here ? (n_it + K - 1) / K : K > 1 ? n_it / K + n_it % K : n_it);
       for (int iter = 0; iter < n_it;) {
-        const int k = (K > 1 && iter + K <= n_it) ? K : 1;
-        if (k > 1) {
+        const int k = cl_here ? std::min(K, n_it - iter) : (K > 1 && iter + K <= n_it) ? K : 1;
+        if (cl_here) {
+          IterCLArgs C = cl_args(variant, sigma, tau, iter, k);
+          C.write_tp = iter + k == n_it;
+          launch_fused_iteration_cluster(C, masked, half, st, variant);
+          for (int j = 0; j < k; j++) {
+            sigma = sigma / C.mu[j];
+            tau = tau * C.mu[j];
+          }
+        } else if (k > 1) {
           IterTBArgs T = tb_args(sigma, tau, iter, k);
           T.write_tp = iter + k == n_it;
           launch_fused_iteration_tb(T, masked, half, st, variant);

@@ -134,6 +134,27 @@ struct IterTBArgs {
 };
 // iterations per launch of an iteration-kernel variant (1 for the one-iteration forms)
 int tb_iterations(int variant);
+
+// ---- up to kCLMaxIters iterations of one small level in one launch of a thread-block
+// cluster that holds the level in shared memory (kernels_cluster.cu) ----
+constexpr int kCLMaxIters = 64;
+struct IterCLArgs {
+  IterPair P;  // pointers of the launch's first iteration
+  float sp[kCLMaxIters], sq[kCLMaxIters], tau[kCLMaxIters], mu[kCLMaxIters];  // per iteration
+  int n;         // iterations (1 .. kCLMaxIters)
+  int parity;    // p / q plane read by the first iteration
+  int write_tp;  // 1: the last iteration stores T p
+  int rows;      // image rows per CTA (cluster_rows)
+};
+// CTAs per cluster of a cluster-resident variant (0 for the other variants)
+int cluster_ctas(int variant);
+// image rows each CTA owns for a level of height h
+int cluster_rows(int variant, int h);
+// the level's state fits the cluster's shared memory and such a cluster can be resident
+bool cluster_fits(int variant, bool masked, bool half, int w, int h);
+double cluster_gpu_share(int variant, int w, int h);
+void launch_fused_iteration_cluster(const IterCLArgs& A, bool masked, bool half_storage, cudaStream_t st,
+                                    int variant);
 // Fraction of the GPU's resident-block capacity that one launch of a variant for one pair of
 // w x h pixels occupies (1 when it fills or exceeds a wave); the tuner's cost model.
 double iteration_gpu_share(int variant, bool masked, bool half, int w, int h);
@@ -258,15 +279,20 @@ inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFT
 // 62 x 4 tiles (kernels_x2.cu); one pair per launch only.
 // variants 12-13: k_fused_iter_tb with one region pixel per thread, 7 iterations on 11 x 11
 // tiles and 9 on 5 x 5 tiles (for the smallest levels, where the GPU is mostly idle).
-constexpr int kIterVariants = 14;
-constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17, 8, 4, 11, 5};
-constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 3, 6, 0, 0};
+// variants 14-15: k_fused_iter_cluster, the whole level in the shared memory of a cluster of
+// 16 / 8 CTAs, all iterations of a warp (up to kCLMaxIters) per launch; levels that do not
+// fit use the default variant.
+constexpr int kIterVariants = 16;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17, 8, 4, 11, 5, 0, 0};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 3, 6, 0, 0, 0, 0};
 constexpr int kIterFirstRowsVariant = 3;
 constexpr int kIterFirstTBVariant = 6;
 constexpr int kIterFirstX2Variant = 10;
 // variants whose launch carries one pair only (others fall back to the default there)
 inline bool iter_variant_single_pair(int v) { return v >= kIterFirstTBVariant; }
 constexpr int kIterFirstDeepTBVariant = 12;
+constexpr int kIterFirstClusterVariant = 14;
+inline bool iter_variant_cluster(int v) { return v >= kIterFirstClusterVariant && v < kIterVariants; }
 constexpr int kIterDefaultVariant = 1;
 inline int iter_tiles_x_of(int w) { return (w + 30) / 31; }
 inline int iter_tiles_of(int w, int h, int rows) { return iter_tiles_x_of(w) * ((h + rows - 1) / rows); }

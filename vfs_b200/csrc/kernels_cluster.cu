@@ -1,0 +1,358 @@
+// Cluster-resident form of the fused primal-dual iteration: all iterations of one warp of a
+// small pyramid level in one launch.
+//
+// One thread-block cluster of C CTAs (16, or the portable 8) holds the whole level in shared
+// memory.  CTA k owns the image rows [k R, k R + R) (R = ceil(h / C)) and keeps them with a
+// one-row halo north and south and the columns -1 .. w (column -1 is the flat position before
+// column 0, the reference's west neighbour of column 0).  One iteration is
+//   * the dual step and T p at the owned pixels; a pixel of the last owned row also stores its
+//     T p and (unrounded) q into the south CTA's north halo row (distributed shared memory);
+//   * a cluster barrier;
+//   * the threshold and primal steps at the owned pixels; a pixel of the first / last owned
+//     row also stores its u-bar and v-bar into the north / south CTA's halo row;
+//   * a cluster barrier.
+// The dual step reads u-bar and v-bar of the pixel and of its east / south (or west / north)
+// neighbours; the threshold and primal steps read T p and q of the pixel and of its west /
+// north neighbours.  The barriers order every halo store between the phase that produces it
+// and the phase that reads it, and after the last iteration no CTA touches another's memory.
+// The per-pixel operations are those of k_fused_iter (region_step.cuh), so the results are
+// bit-identical to one launch per iteration: no halo pixel is recomputed, no launch is made
+// per iteration, and the level's state never leaves the chip between iterations.
+//
+// Pixels that an iteration leaves unwritten (masked out, and column -1) alternate between the
+// values the two ping-pong buffers hold; the CTA keeps both and swaps them after each
+// iteration.  At the end the owned active pixels are written into the buffers that hold the
+// current state after n iterations: the other ping-pong buffers for odd n, the launch's
+// input buffers for even n.  The values the other buffers would hold are those of the
+// iteration before the last, which no later step reads: every iteration writes them before
+// anything reads them.
+//
+// When the level has no row padding (stride == width), column -1 of a row is the previous
+// row's last pixel, which changes every iteration; the caller then uses this kernel only if
+// no pixel of column 0 is on (StereoTgvImpl::tb_ok), as for the temporally blocked form.
+#include "common.cuh"
+#include "fused.cuh"
+#include "region_step.cuh"
+
+#include <cooperative_groups.h>
+
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <tuple>
+
+namespace vfs {
+
+namespace cg = cooperative_groups;
+
+namespace {
+
+constexpr int kMaxDevices = 64;
+constexpr int kCLMaxThreads = 1024;
+constexpr int kCLMaxPixelsPerThread = 3;
+
+struct CLGeometry {
+  int rows = 0;         // image rows per CTA
+  int rx = 0, ry = 0;   // region columns (w + 2) and rows (rows + 2)
+  int n = 0;            // elements per array (a multiple of 4)
+  size_t bytes = 0;     // dynamic shared memory per CTA
+  int ppt = 0;          // owned pixels per thread (1 .. kCLMaxPixelsPerThread)
+  int threads = 0;      // threads per CTA
+};
+
+template <class ST>
+CLGeometry cl_geometry(int ctas, int w, int h) {
+  CLGeometry g;
+  g.rows = (h + ctas - 1) / ctas;
+  g.rx = w + 2;
+  g.ry = g.rows + 2;
+  g.n = ((g.rx * g.ry + 3) / 4) * 4;
+  g.bytes = (size_t)g.n * RegionState<ST>::kBytesPerPixel;
+  const int px = g.rows * w;
+  for (int k = 1; k <= kCLMaxPixelsPerThread; k++) {
+    const int t = ((px + k - 1) / k + 31) / 32 * 32;
+    if (t <= kCLMaxThreads) {
+      g.ppt = k;
+      g.threads = t;
+      break;
+    }
+  }
+  return g;
+}
+
+}  // namespace
+
+// PPT: owned pixels per thread (thread t owns the owned-pixel indices t + k blockDim.x).
+template <bool MASKED, class ST, int PPT>
+__global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const __grid_constant__ IterCLArgs A) {
+  typedef Store2<ST> S;
+  typedef typename S::T2 T2;
+  typedef typename S::T4 T4;
+  extern __shared__ __align__(16) unsigned char smem[];
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+
+  const IterPair& P = A.P;
+  const int w = P.w, h = P.h, s = P.s;
+  const int rows = A.rows, RX = w + 2, RY = rows + 2, N = ((RX * RY + 3) / 4) * 4;
+  const int r0 = rank * rows;                                // first owned row
+  const int nown = max(0, min(rows, h - r0));                // owned rows (0 for trailing CTAs)
+  const bool north = rank > 0 && nown > 0;                   // a CTA owns the rows above
+  const bool south = nown == rows && r0 + rows < h;          // a CTA owns the rows below
+  RegionState<ST> R;
+  R.carve(smem, N);
+  // a halo value goes to the same array element of a neighbour (every CTA has the same layout)
+  auto to = [&](auto* local, int rank_to) { return cl.map_shared_rank(local, (unsigned)rank_to); };
+
+  const int plane = s * h;
+  const T2* pin = (const T2*)P.p + (A.parity ? plane : 0);
+  const T4* qin = (const T4*)P.q + (A.parity ? plane : 0);
+  const int tid = (int)threadIdx.x, nthr = (int)blockDim.x;
+  griddep_wait();
+
+  // ---- load the owned rows and the halo rows -------------------------------------------
+  if (nown > 0)
+    for (int l = tid; l < RX * (nown + 2); l += nthr) {
+      const int ry = l / RX, rx = l - ry * RX;
+      R.template load<MASKED>(P, pin, qin, ry * RX + rx, rx - 1, r0 - 1 + ry);
+    }
+  // this thread's owned pixels: region index (< 0: none) and image column | row << 16
+  int pi[PPT], pxy[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; k++) {
+    const int l = tid + k * nthr;
+    const int ry = l / max(w, 1), rx = l - ry * w;
+    const bool own = l < nown * w;
+    pi[k] = own ? (ry + 1) * RX + rx + 1 : -1;
+    pxy[k] = own ? rx | ((r0 + ry) << 16) : 0;
+  }
+  const int last_row = r0 + nown - 1;
+  __syncthreads();
+
+#pragma unroll 1
+  for (int j = 0; j < A.n; j++) {
+    // ---- dual step; the last owned row's T p and q go to the south CTA's halo ----------
+    // (one copy of the per-pixel code: under the 64-register limit of 1024-thread CTAs
+    // unrolled copies spill)
+#pragma unroll 1
+    for (int k = 0; k < PPT; k++) {
+      const int i = pi[k];
+      if (i < 0) continue;
+      const int gx = pxy[k] & 0xffff, gy = pxy[k] >> 16;
+      if (R.template dual<MASKED>(i, RX, gx, gy, w, h, A.sp[j], A.sq[j]) && south && gy == last_row) {
+        const int hi = i - nown * RX;  // row 0 of the south CTA's region
+        *to(R.tp + hi, rank + 1) = R.tp[i];
+        *to(R.q + hi, rank + 1) = R.q[i];
+      }
+    }
+    cl.sync();
+    // ---- threshold and primal steps; u-bar and v-bar of the edge rows to the halos -------
+#pragma unroll 1
+    for (int k = 0; k < PPT; k++) {
+      const int i = pi[k];
+      if (i < 0) continue;
+      const int gx = pxy[k] & 0xffff, gy = pxy[k] >> 16;
+      if (MASKED && !(R.code[i] & kOn)) R.keep(i);
+      else R.template primal<MASKED>(P, i, RX, gx, gy, A.tau[j], A.mu[j]);
+      if (north && gy == r0) {
+        const int hi = i + rows * RX;  // row rows + 1 of the north CTA's region
+        *to(R.ub + hi, rank - 1) = R.ub[i];
+        *to(R.v + hi, rank - 1) = R.v[i];
+      }
+      if (south && gy == last_row) {
+        const int hi = i - nown * RX;
+        *to(R.ub + hi, rank + 1) = R.ub[i];
+        *to(R.v + hi, rank + 1) = R.v[i];
+      }
+    }
+    // column -1 of the owned rows is never written: it alternates like a masked-out pixel
+    if (MASKED && tid < nown) R.keep((tid + 1) * RX);
+    cl.sync();
+  }
+
+  // ---- write the owned active pixels into the buffers current after n iterations --------
+  const bool odd = A.n & 1;
+  float* uo = odd ? P.us : const_cast<float*>(P.u);
+  float* ubo = odd ? P.u_s : const_cast<float*>(P.u_);
+  T2* vo = (T2*)(odd ? P.v_s : const_cast<void*>(P.v_));
+  const int pl = (A.parity + A.n) & 1;  // p / q plane written by the last iteration
+  T2* po = (T2*)P.p + (pl ? plane : 0);
+  T4* qo = (T4*)P.q + (pl ? plane : 0);
+#pragma unroll
+  for (int k = 0; k < PPT; k++) {
+    const int i = pi[k];
+    if (i < 0) continue;
+    if (MASKED && !(R.code[i] & kOn)) continue;
+    const int pos = (pxy[k] & 0xffff) + (pxy[k] >> 16) * s;
+    uo[pos] = R.u[i];
+    ubo[pos] = R.ub[i];
+    vo[pos] = R.v[i];
+    po[pos] = R.p[i];
+    qo[pos] = S::rnd4(R.q[i]);
+    if (A.write_tp) P.Tp[pos] = R.tp[i];
+  }
+}
+
+namespace {
+
+template <bool MASKED, class ST, int PPT>
+void set_cl_attributes() {
+  auto k = k_fused_iter_cluster<MASKED, ST, PPT>;
+  static std::atomic<bool> configured[kMaxDevices];
+  int dev = 0;
+  VFS_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < kMaxDevices && configured[dev].load(std::memory_order_acquire)) return;
+  int optin = 0;
+  VFS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  VFS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  VFS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+  if (dev >= 0 && dev < kMaxDevices) configured[dev].store(true, std::memory_order_release);
+}
+
+template <bool MASKED, class ST, int PPT>
+cudaLaunchConfig_t cl_config(const CLGeometry& g, int ctas, cudaStream_t st, cudaLaunchAttribute* at,
+                             unsigned& nat) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(ctas);
+  cfg.blockDim = dim3(g.threads);
+  cfg.dynamicSmemBytes = g.bytes;
+  cfg.stream = st;
+  nat = 0;
+  at[nat].id = cudaLaunchAttributeClusterDimension;
+  at[nat].val.clusterDim.x = ctas;
+  at[nat].val.clusterDim.y = 1;
+  at[nat].val.clusterDim.z = 1;
+  nat++;
+  cfg.attrs = at;
+  cfg.numAttrs = nat;
+  return cfg;
+}
+
+// can a cluster of this shape be resident on the device (0 or the number of such clusters)
+template <bool MASKED, class ST, int PPT>
+int cl_max_clusters(const CLGeometry& g, int ctas) {
+  set_cl_attributes<MASKED, ST, PPT>();
+  cudaLaunchAttribute at[2];
+  unsigned nat = 0;
+  cudaLaunchConfig_t cfg = cl_config<MASKED, ST, PPT>(g, ctas, 0, at, nat);
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k_fused_iter_cluster<MASKED, ST, PPT>, &cfg) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+template <bool MASKED, class ST>
+int cl_max_clusters_ppt(const CLGeometry& g, int ctas) {
+  switch (g.ppt) {
+    case 1: return cl_max_clusters<MASKED, ST, 1>(g, ctas);
+    case 2: return cl_max_clusters<MASKED, ST, 2>(g, ctas);
+    case 3: return cl_max_clusters<MASKED, ST, 3>(g, ctas);
+    default: return 0;
+  }
+}
+
+template <bool MASKED, class ST, int PPT>
+void launch_cl(const IterCLArgs& A, const CLGeometry& g, int ctas, cudaStream_t st) {
+  set_cl_attributes<MASKED, ST, PPT>();
+  cudaLaunchAttribute at[2];
+  unsigned nat = 0;
+  cudaLaunchConfig_t cfg = cl_config<MASKED, ST, PPT>(g, ctas, st, at, nat);
+  const int prio = launch_priority();
+  if (prio != 0) {
+    at[nat].id = cudaLaunchAttributePriority;
+    at[nat].val.priority = prio;
+    nat++;
+    cfg.numAttrs = nat;
+  }
+  VFS_CUDA(cudaLaunchKernelEx(&cfg, k_fused_iter_cluster<MASKED, ST, PPT>, A));
+}
+
+template <bool MASKED, class ST>
+void launch_cl_ppt(const IterCLArgs& A, const CLGeometry& g, int ctas, cudaStream_t st) {
+  switch (g.ppt) {
+    case 1: launch_cl<MASKED, ST, 1>(A, g, ctas, st); break;
+    case 2: launch_cl<MASKED, ST, 2>(A, g, ctas, st); break;
+    case 3: launch_cl<MASKED, ST, 3>(A, g, ctas, st); break;
+    default: throw ArgError{"cluster-resident iteration: level too large"};
+  }
+}
+
+CLGeometry geometry_of(bool half, int ctas, int w, int h) {
+  return half ? cl_geometry<__half>(ctas, w, h) : cl_geometry<float>(ctas, w, h);
+}
+
+}  // namespace
+
+int cluster_ctas(int variant) {
+  switch (variant) {
+    case kIterFirstClusterVariant: return 16;
+    case kIterFirstClusterVariant + 1: return 8;
+    default: return 0;
+  }
+}
+
+bool cluster_fits(int variant, bool masked, bool half, int w, int h) {
+  const int ctas = cluster_ctas(variant);
+  if (ctas <= 0 || w <= 0 || h <= 0) return false;
+  int dev = 0;
+  VFS_CUDA(cudaGetDevice(&dev));
+  // the answer depends only on the device and the shape; ask the runtime once per shape
+  static std::mutex mu;
+  static std::map<std::tuple<int, int, bool, bool, int, int>, bool> known;
+  const auto key = std::make_tuple(dev, ctas, masked, half, w, h);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = known.find(key);
+    if (it != known.end()) return it->second;
+  }
+  const CLGeometry g = geometry_of(half, ctas, w, h);
+  int optin = 0;
+  VFS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  bool ok = g.ppt > 0 && g.bytes <= (size_t)optin && w + 2 <= 4096;
+  if (ok) {
+    int n = 0;
+    if (masked) n = half ? cl_max_clusters_ppt<true, __half>(g, ctas) : cl_max_clusters_ppt<true, float>(g, ctas);
+    else n = half ? cl_max_clusters_ppt<false, __half>(g, ctas) : cl_max_clusters_ppt<false, float>(g, ctas);
+    ok = n >= 1;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  known[key] = ok;
+  return ok;
+}
+
+int cluster_rows(int variant, int h) {
+  const int ctas = cluster_ctas(variant);
+  return ctas > 0 ? (h + ctas - 1) / ctas : 0;
+}
+
+double cluster_gpu_share(int variant, int w, int h) {
+  (void)w;
+  (void)h;
+  int dev = 0, sms = 1;
+  VFS_CUDA(cudaGetDevice(&dev));
+  VFS_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  // one CTA per SM (the level's state takes most of an SM's shared memory or threads)
+  return std::min(1.0, (double)cluster_ctas(variant) / (double)sms);
+}
+
+void launch_fused_iteration_cluster(const IterCLArgs& A, bool masked, bool half_storage, cudaStream_t st,
+                                    int variant) {
+  const int ctas = cluster_ctas(variant);
+  if (ctas <= 0) throw ArgError{"not a cluster-resident iteration variant"};
+  if (A.n < 1 || A.n > kCLMaxIters) throw ArgError{"cluster-resident iteration: bad iteration count"};
+  if (A.P.w <= 0 || A.P.h <= 0) return;
+  const CLGeometry g = geometry_of(half_storage, ctas, A.P.w, A.P.h);
+  if (A.rows != g.rows || g.ppt == 0) throw ArgError{"cluster-resident iteration: bad geometry"};
+  if (masked) {
+    if (half_storage) launch_cl_ppt<true, __half>(A, g, ctas, st);
+    else launch_cl_ppt<true, float>(A, g, ctas, st);
+  } else {
+    if (half_storage) launch_cl_ppt<false, __half>(A, g, ctas, st);
+    else launch_cl_ppt<false, float>(A, g, ctas, st);
+  }
+  VFS_LAUNCH_CHECK();
+}
+
+}  // namespace vfs

@@ -281,7 +281,9 @@ double iteration_gpu_share(int variant, bool masked, bool half, int w, int h) {
   // blocks of the launch and resident blocks per SM of the variant's kernel (one pair)
   long long blocks = 0;
   int per_sm = 0;
-  if (variant >= kIterFirstX2Variant && variant < kIterFirstDeepTBVariant) {
+  if (iter_variant_cluster(variant)) {
+    return cluster_gpu_share(variant, w, h);
+  } else if (variant >= kIterFirstX2Variant && variant < kIterFirstDeepTBVariant) {
     return x2_gpu_share(variant, masked, half, w, h);
   } else if (variant >= kIterFirstTBVariant) {
     return tb_gpu_share(variant, masked, half, w, h);

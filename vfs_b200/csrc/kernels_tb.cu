@@ -24,11 +24,9 @@
 // column 0 is on (StereoTgvImpl::tb_ok).
 #include "common.cuh"
 #include "fused.cuh"
-#include "tgv_pixel.cuh"
-#include "tgv_pixel_fast.cuh"
+#include "region_step.cuh"
 
 #include <atomic>
-#include <type_traits>
 
 namespace vfs {
 
@@ -39,16 +37,9 @@ constexpr int kMaxDevices = 64;
 
 template <class ST, int K, int TX, int TY>
 struct TBLayout {
-  typedef typename Store2<ST>::T2 T2;
-  typedef typename Store2<ST>::T4 T4;
   static constexpr int RX = TX + 3 * K, RY = TY + 3 * K;
   static constexpr int N = ((RX * RY + 3) / 4) * 4;  // elements per array (16-byte aligned arrays)
-  // float arrays: ubar, ubar_alt, u, a, b, c, Iu, Iz; T2: v, v_alt, p; float4: q; float2: Tp;
-  // u8: code.  q is kept unrounded: within an iteration the threshold and primal steps read
-  // this iteration's q at full precision (as the one-iteration kernel does from registers and
-  // shared memory); the next iteration's dual step reads it in the stored precision.
-  static constexpr size_t kBytes =
-      (size_t)N * (8 * sizeof(float) + 3 * sizeof(T2) + sizeof(float4) + sizeof(float2) + 1);
+  static constexpr size_t kBytes = (size_t)N * RegionState<ST>::kBytesPerPixel;
 };
 
 }  // namespace
@@ -59,26 +50,13 @@ template <bool MASKED, class ST, int K, int TX, int TY, int BY>
 __global__ void __launch_bounds__(kTBX* BY, 1) k_fused_iter_tb(const __grid_constant__ IterTBArgs A) {
   constexpr int kTBY = BY;
   typedef TBLayout<ST, K, TX, TY> L;
-  typedef typename L::T2 T2;
-  typedef typename L::T4 T4;
   typedef Store2<ST> S;
-  constexpr int RX = L::RX, RY = L::RY, N = L::N;
-  constexpr bool kFast = !std::is_same<ST, float>::value;
+  typedef typename S::T2 T2;
+  typedef typename S::T4 T4;
+  constexpr int RX = L::RX, RY = L::RY;
   extern __shared__ __align__(16) unsigned char smem[];
-  float* s_ub = reinterpret_cast<float*>(smem);
-  float* s_uba = s_ub + N;
-  float* s_u = s_uba + N;
-  float* s_a = s_u + N;
-  float* s_b = s_a + N;
-  float* s_c = s_b + N;
-  float* s_Iu = s_c + N;
-  float* s_Iz = s_Iu + N;
-  T2* s_v = reinterpret_cast<T2*>(s_Iz + N);
-  T2* s_va = s_v + N;
-  T2* s_p = s_va + N;
-  float4* s_q = reinterpret_cast<float4*>(s_p + N);
-  float2* s_tp = reinterpret_cast<float2*>(s_q + N);
-  uint8_t* s_code = reinterpret_cast<uint8_t*>(s_tp + N);
+  RegionState<ST> R;
+  R.carve(smem, L::N);
 
   const IterPair& P = A.P;
   const int w = P.w, h = P.h, s = P.s;
@@ -88,96 +66,25 @@ __global__ void __launch_bounds__(kTBX* BY, 1) k_fused_iter_tb(const __grid_cons
   const T4* qin = (const T4*)P.q + (A.parity ? plane : 0);
   T2* pout = (T2*)P.p + (A.parity ? 0 : plane);
   T4* qout = (T4*)P.q + (A.parity ? 0 : plane);
-  const T2* vin = (const T2*)P.v_;
-  const T2* valt = (const T2*)P.v_s;  // the other ping-pong buffer of v-bar (also the output)
   const int tx = threadIdx.x, ty = threadIdx.y;
   griddep_wait();  // the previous launch's outputs are this one's inputs
   griddep_launch_dependents();
 
   // ---- load the region --------------------------------------------------------------
-  for (int ry = ty; ry < RY; ry += kTBY) {
-    const int gy = gy0 + ry;
-    for (int rx = tx; rx < RX; rx += kTBX) {
-      const int gx = gx0 + rx;
-      const int i = ry * RX + rx;
-      const int pos = gx + gy * s;
-      const bool in = gx >= 0 && gx < w && gy >= 0 && gy < h;
-      // flat positions the reference may read: columns [-1, w) of rows < h, at or after the
-      // buffer start (column -1 is the previous row's last padding element)
-      const bool flat = gx >= -1 && gx < w && gy < h && pos >= 0;
-      const uint8_t code = in ? P.code[pos] : (uint8_t)0;
-      const bool act = MASKED ? (in && (code & kOn)) : in;  // written by every iteration
-      s_code[i] = code;
-      s_ub[i] = flat ? P.u_[pos] : 0.0f;
-      s_v[i] = flat ? vin[pos] : S::ld2z();
-      if (MASKED) {
-        s_uba[i] = (flat && !act) ? P.u_s[pos] : 0.0f;
-        s_va[i] = (flat && !act) ? valt[pos] : S::ld2z();
-      }
-      s_u[i] = act ? P.u[pos] : 0.0f;
-      s_p[i] = act ? pin[pos] : S::ld2z();
-      s_q[i] = act ? S::cvt4(qin[pos]) : make_float4(0.f, 0.f, 0.f, 0.f);
-      s_a[i] = in ? P.a[pos] : 0.0f;
-      s_b[i] = in ? P.b[pos] : 0.0f;
-      s_c[i] = in ? P.c[pos] : 0.0f;
-      s_Iu[i] = act ? P.Iu[pos] : 0.0f;
-      s_Iz[i] = act ? P.Iz[pos] : 0.0f;
-      // stored T p: read where a pixel keeps its values (masked form) and west of column 0
-      const bool tps = (MASKED && in && !act) || (gx == -1 && gy >= 1 && gy < h);
-      s_tp[i] = tps ? P.Tp[pos] : make_float2(0.f, 0.f);
-    }
-  }
+  for (int ry = ty; ry < RY; ry += kTBY)
+    for (int rx = tx; rx < RX; rx += kTBX) R.template load<MASKED>(P, pin, qin, ry * RX + rx, gx0 + rx, gy0 + ry);
   __syncthreads();
 
 #pragma unroll 1
   for (int j = 0; j < K; j++) {
-    const float sp = A.sp[j], sq = A.sq[j], tau = A.tau[j], mu = A.mu[j];
     // ---- dual step on D_j ----------------------------------------------------------------
     const int dlo = 2 * j + 1, dhx = RX - (j + 1), dhy = RY - (j + 1);
     for (int ry = dlo + ty; ry < dhy; ry += kTBY) {
       const int gy = gy0 + ry;
       for (int rx = dlo + tx; rx < dhx; rx += kTBX) {
         const int gx = gx0 + rx;
-        const int i = ry * RX + rx;
-        const uint8_t code = s_code[i];
-        const bool in = gx >= 0 && gx < w && gy >= 0 && gy < h;
-        if (!in) continue;
-        bool useRight, useDown;
-        const float a = s_a[i], b = s_b[i], c = s_c[i];
-        if (MASKED) {
-          if (!(code & kOn)) continue;  // keeps its values; its stored T p is in s_tp
-          useRight = code & kR;
-          useDown = code & kD;
-        } else {
-          if (!(code & kOn)) {  // outside the circle: p = q = 0, T p = T 0
-            const float2 z = make_float2(0.f, 0.f);
-            s_p[i] = S::ld2z();
-            s_q[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            s_tp[i] = kFast ? fast::tp(a, b, c, z) : tp_math(a, b, c, z);
-            continue;
-          }
-          useRight = (gx + 1) < w;
-          useDown = (gy + 1) < h;
-        }
-        const float ubar = s_ub[i];
-        const float2 vb = S::cvt2(s_v[i]);
-        const float u_xn = useRight ? s_ub[i + 1] : s_ub[i - 1];
-        const float u_yn = useDown ? s_ub[i + RX] : s_ub[i - RX];
-        const float2 v_xn = S::cvt2(useRight ? s_v[i + 1] : s_v[i - 1]);
-        const float2 v_yn = S::cvt2(useDown ? s_v[i + RX] : s_v[i - RX]);
-        float2 pp = S::cvt2(s_p[i]);
-        float4 qq = S::cvt4(S::rnd4(s_q[i]));  // the stored (rounded) q of the last iteration
-        float2 tp;
-        if (kFast) {
-          fast::dual(useRight, useDown, ubar, u_xn, u_yn, vb, v_xn, v_yn, a, b, c, sp, sq, pp, qq);
-          tp = fast::tp(a, b, c, pp);
-        } else {
-          dual_math(useRight, useDown, ubar, u_xn, u_yn, vb, v_xn, v_yn, a, b, c, sp, sq, pp, qq);
-          tp = tp_math(a, b, c, pp);
-        }
-        s_p[i] = S::rnd2(pp);
-        s_q[i] = qq;
-        s_tp[i] = tp;
+        if (!(gx >= 0 && gx < w && gy >= 0 && gy < h)) continue;
+        R.template dual<MASKED>(ry * RX + rx, RX, gx, gy, w, h, A.sp[j], A.sq[j]);
       }
     }
     __syncthreads();
@@ -188,85 +95,14 @@ __global__ void __launch_bounds__(kTBX* BY, 1) k_fused_iter_tb(const __grid_cons
       for (int rx = tx; rx < RX; rx += kTBX) {
         const int gx = gx0 + rx;
         const int i = ry * RX + rx;
-        const uint8_t code = s_code[i];
         const bool in = gx >= 0 && gx < w && gy >= 0 && gy < h;
-        const bool act = MASKED ? (in && (code & kOn)) : in;
+        const bool act = MASKED ? (in && (R.code[i] & kOn)) : in;
         if (!act) {
-          if (MASKED) {
-            const float t = s_ub[i];
-            s_ub[i] = s_uba[i];
-            s_uba[i] = t;
-            const T2 tv = s_v[i];
-            s_v[i] = s_va[i];
-            s_va[i] = tv;
-          }
+          if (MASKED) R.keep(i);
           continue;
         }
         if (rx < olo || rx >= ohx || ry < olo || ry >= ohy) continue;
-        float dxm, dym;
-        bool zR, zD, hasL, hasU;
-        const float2 tp = s_tp[i], tpW = s_tp[i - 1], tpN = s_tp[i - RX];
-        if (MASKED) {
-          const bool mR = code & kR, mL = code & kL, mD = code & kD, mU = code & kU;
-          if (mL && mR) dxm = tp.x - tpW.x;
-          else if (!mR) dxm = -tpW.x;
-          else dxm = tp.x;
-          if (mU && mD) dym = tp.y - tpN.y;
-          else if (!mD) dym = -tpN.y;
-          else dym = tp.y;
-          zR = !mR;
-          zD = !mD;
-          hasL = mL;
-          hasU = mU;
-        } else {
-          if (!(code & kOn)) {
-            s_u[i] = 0.0f;
-            s_ub[i] = 0.0f;
-            s_v[i] = S::rnd2(make_float2(0.f, 0.f));
-            continue;
-          }
-          if ((gx - 1) >= 0) dxm = tp.x - tpW.x;
-          else if (gx == w - 1) dxm = -tpW.x;
-          else dxm = tp.x;
-          if ((gy - 1) >= 0) dym = tp.y - tpN.y;
-          else if (gy == h - 1) dym = -tpN.y;
-          else dym = tp.y;
-          zR = gx == w - 1;
-          zD = gy == h - 1;
-          hasL = (gx - 1) >= 0;
-          hasU = (gy - 1) >= 0;
-        }
-        const float a = s_a[i], b = s_b[i], c = s_c[i];
-        const float ubar = s_ub[i];
-        const float2 vb = S::cvt2(s_v[i]);
-        float unew;
-        if (kFast) {
-          float eu = fast::etau(a, b, c, P.alpha1 * P.alpha1);
-          unew = fast::threshold(dxm, dym, eu, tau, ubar, s_u[i], s_Iu[i], s_Iz[i], P.lambda);
-        } else {
-          float eu = etau_math(a, b, c, P.alpha1);
-          unew = threshold_math(dxm, dym, eu, tau, ubar, s_u[i], s_Iu[i], s_Iz[i], P.lambda);
-        }
-        float4 qc = s_q[i];
-        if (zR) qc.x = qc.w = 0.0f;
-        if (zD) qc.y = qc.z = 0.0f;
-        const float4 ql = hasL ? s_q[i - 1] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 qu = hasU ? s_q[i - RX] : make_float4(0.f, 0.f, 0.f, 0.f);
-        float us_;
-        float2 vs;
-        if (kFast) {
-          const float a1s = P.alpha1 * P.alpha1, a0s4 = 4.0f * P.alpha0 * P.alpha0;
-          float ev1 = fast::etav(b, c, a1s, a0s4), ev2 = fast::etav(a, c, a1s, a0s4);
-          fast::primal(qc, ql, qu, tp, ev1, ev2, tau, P.alpha0, P.alpha1, mu, vb, unew, ubar, us_, vs);
-        } else {
-          float ev1 = etav1_math(b, c, P.alpha0, P.alpha1), ev2 = etav2_math(a, c, P.alpha0, P.alpha1);
-          float2 vo;
-          const float2 pp = S::cvt2(s_p[i]);
-          primal_math(qc, ql, qu, pp, a, b, c, ev1, ev2, tau, P.alpha0, P.alpha1, mu, vb, unew, ubar, us_, vs, vo);
-        }
-        s_u[i] = unew;
-        s_ub[i] = us_;
-        s_v[i] = S::rnd2(vs);
+        R.template primal<MASKED>(P, i, RX, gx, gy, A.tau[j], A.mu[j]);
       }
     }
     __syncthreads();
@@ -280,15 +116,14 @@ __global__ void __launch_bounds__(kTBX* BY, 1) k_fused_iter_tb(const __grid_cons
       const int gx = gx0 + rx;
       if (gx >= w) break;
       const int i = ry * RX + rx;
-      const uint8_t code = s_code[i];
-      if (MASKED && !(code & kOn)) continue;
+      if (MASKED && !(R.code[i] & kOn)) continue;
       const int pos = gx + gy * s;
-      P.us[pos] = s_u[i];
-      P.u_s[pos] = s_ub[i];
-      ((T2*)P.v_s)[pos] = s_v[i];
-      pout[pos] = s_p[i];
-      qout[pos] = S::rnd4(s_q[i]);
-      if (A.write_tp) P.Tp[pos] = s_tp[i];
+      P.us[pos] = R.u[i];
+      P.u_s[pos] = R.ub[i];
+      ((T2*)P.v_s)[pos] = R.v[i];
+      pout[pos] = R.p[i];
+      qout[pos] = S::rnd4(R.q[i]);
+      if (A.write_tp) P.Tp[pos] = R.tp[i];
     }
   }
 }
