@@ -166,7 +166,8 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
       }
     }
     // column -1 of the owned rows is never written: it alternates like a masked-out pixel
-    if (MASKED && tid < nown) R.keep((tid + 1) * RX);
+    if (MASKED)
+      for (int r = tid; r < nown; r += nthr) R.keep((r + 1) * RX);
     cl.sync();
   }
 
@@ -310,7 +311,8 @@ bool cluster_fits(int variant, bool masked, bool half, int w, int h) {
   const CLGeometry g = geometry_of(half, ctas, w, h);
   int optin = 0;
   VFS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  bool ok = g.ppt > 0 && g.bytes <= (size_t)optin && w + 2 <= 4096;
+  // (a thread packs a pixel's column and row into one int: 16 bits each)
+  bool ok = g.ppt > 0 && g.bytes <= (size_t)optin && w + 2 <= 4096 && h < 32768;
   if (ok) {
     int n = 0;
     if (masked) n = half ? cl_max_clusters_ppt<true, __half>(g, ctas) : cl_max_clusters_ppt<true, float>(g, ctas);
