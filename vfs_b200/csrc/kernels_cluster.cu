@@ -14,7 +14,9 @@
 // The dual step reads u-bar and v-bar of the pixel and of its east / south (or west / north)
 // neighbours; the threshold and primal steps read T p and q of the pixel and of its west /
 // north neighbours.  The barriers order every halo store between the phase that produces it
-// and the phase that reads it, and after the last iteration no CTA touches another's memory.
+// and the phase that reads it.  A cluster barrier after the initial load keeps the first
+// halo stores from landing before a neighbour has started or has loaded its halo rows from
+// global memory, and after the last iteration no CTA touches another's memory.
 // The per-pixel operations are those of k_fused_iter (region_step.cuh), so the results are
 // bit-identical to one launch per iteration: no halo pixel is recomputed, no launch is made
 // per iteration, and the level's state never leaves the chip between iterations.
@@ -127,7 +129,10 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
     pxy[k] = own ? rx | ((r0 + ry) << 16) : 0;
   }
   const int last_row = r0 + nown - 1;
-  __syncthreads();
+  // A cluster barrier, not a CTA barrier: every CTA of the cluster must have started and
+  // finished loading its halo rows before a neighbour stores the first iteration's values
+  // into them.
+  cl.sync();
 
 #pragma unroll 1
   for (int j = 0; j < A.n; j++) {
