@@ -264,6 +264,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         C.parity = iter0 & 1;
         C.write_tp = 0;
         C.rows = cluster_rows(variant_, C.P.h);
+        C.ctas = cluster_ctas(variant_);
         return C;
       };
       const int lw = act[0]->pW[level], lh = act[0]->pH[level];

@@ -145,6 +145,7 @@ struct IterCLArgs {
   int parity;    // p / q plane read by the first iteration
   int write_tp;  // 1: the last iteration stores T p
   int rows;      // image rows per CTA (cluster_rows)
+  int ctas;      // CTAs of the cluster (cluster_ctas); the grid is one cluster
 };
 // CTAs per cluster of a cluster-resident variant (0 for the other variants)
 int cluster_ctas(int variant);

@@ -36,16 +36,12 @@
 #include "fused.cuh"
 #include "region_step.cuh"
 
-#include <cooperative_groups.h>
-
 #include <atomic>
 #include <map>
 #include <mutex>
 #include <tuple>
 
 namespace vfs {
-
-namespace cg = cooperative_groups;
 
 namespace {
 
@@ -82,6 +78,49 @@ CLGeometry cl_geometry(int ctas, int w, int h) {
   return g;
 }
 
+// ---- cluster primitives, in PTX with memory clobbers so that the compiler keeps every
+// shared-memory access on its side of a barrier ----
+
+// All threads of all CTAs of the cluster: stores before it (local and remote) are visible
+// to every thread of the cluster after it.
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile(
+      "barrier.cluster.arrive.release.aligned;\n\t"
+      "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ unsigned cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cluster_size() {
+  unsigned n;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(n));
+  return n;
+}
+// the shared::cluster address of the same shared-memory element in CTA `rank`
+__device__ __forceinline__ unsigned cluster_addr(const void* local, unsigned rank) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(local);
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, float v) {
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, float2 v) {
+  asm volatile("st.shared::cluster.v2.f32 [%0], {%1, %2};" ::"r"(addr), "f"(v.x), "f"(v.y) : "memory");
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, float4 v) {
+  asm volatile("st.shared::cluster.v4.f32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "f"(v.x), "f"(v.y), "f"(v.z),
+               "f"(v.w)
+               : "memory");
+}
+__device__ __forceinline__ void st_cluster(unsigned addr, __half2 v) {
+  const unsigned b = *reinterpret_cast<const unsigned*>(&v);
+  asm volatile("st.shared::cluster.b32 [%0], %1;" ::"r"(addr), "r"(b) : "memory");
+}
+
 }  // namespace
 
 // PPT: owned pixels per thread (thread t owns the owned-pixel indices t + k blockDim.x).
@@ -91,8 +130,11 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
   typedef typename S::T2 T2;
   typedef typename S::T4 T4;
   extern __shared__ __align__(16) unsigned char smem[];
-  cg::cluster_group cl = cg::this_cluster();
-  const int rank = (int)cl.block_rank();
+  const int rank = (int)cluster_rank();
+  // The grid must be exactly one cluster of A.ctas CTAs; any other shape would address CTAs
+  // that do not exist.  The test is the same for every CTA, so all of them leave together,
+  // before any barrier or distributed-shared-memory access.
+  if ((int)cluster_size() != A.ctas || (int)(gridDim.x * gridDim.y * gridDim.z) != A.ctas) return;
 
   const IterPair& P = A.P;
   const int w = P.w, h = P.h, s = P.s;
@@ -104,7 +146,7 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
   RegionState<ST> R;
   R.carve(smem, N);
   // a halo value goes to the same array element of a neighbour (every CTA has the same layout)
-  auto to = [&](auto* local, int rank_to) { return cl.map_shared_rank(local, (unsigned)rank_to); };
+  auto to = [](const void* local, int rank_to) { return cluster_addr(local, (unsigned)rank_to); };
 
   const int plane = s * h;
   const T2* pin = (const T2*)P.p + (A.parity ? plane : 0);
@@ -132,7 +174,7 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
   // A cluster barrier, not a CTA barrier: every CTA of the cluster must have started and
   // finished loading its halo rows before a neighbour stores the first iteration's values
   // into them.
-  cl.sync();
+  cluster_barrier();
 
 #pragma unroll 1
   for (int j = 0; j < A.n; j++) {
@@ -146,11 +188,11 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
       const int gx = pxy[k] & 0xffff, gy = pxy[k] >> 16;
       if (R.template dual<MASKED>(i, RX, gx, gy, w, h, A.sp[j], A.sq[j]) && south && gy == last_row) {
         const int hi = i - nown * RX;  // row 0 of the south CTA's region
-        *to(R.tp + hi, rank + 1) = R.tp[i];
-        *to(R.q + hi, rank + 1) = R.q[i];
+        st_cluster(to(R.tp + hi, rank + 1), R.tp[i]);
+        st_cluster(to(R.q + hi, rank + 1), R.q[i]);
       }
     }
-    cl.sync();
+    cluster_barrier();
     // ---- threshold and primal steps; u-bar and v-bar of the edge rows to the halos -------
 #pragma unroll 1
     for (int k = 0; k < PPT; k++) {
@@ -161,19 +203,19 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
       else R.template primal<MASKED>(P, i, RX, gx, gy, A.tau[j], A.mu[j]);
       if (north && gy == r0) {
         const int hi = i + rows * RX;  // row rows + 1 of the north CTA's region
-        *to(R.ub + hi, rank - 1) = R.ub[i];
-        *to(R.v + hi, rank - 1) = R.v[i];
+        st_cluster(to(R.ub + hi, rank - 1), R.ub[i]);
+        st_cluster(to(R.v + hi, rank - 1), R.v[i]);
       }
       if (south && gy == last_row) {
         const int hi = i - nown * RX;
-        *to(R.ub + hi, rank + 1) = R.ub[i];
-        *to(R.v + hi, rank + 1) = R.v[i];
+        st_cluster(to(R.ub + hi, rank + 1), R.ub[i]);
+        st_cluster(to(R.v + hi, rank + 1), R.v[i]);
       }
     }
     // column -1 of the owned rows is never written: it alternates like a masked-out pixel
     if (MASKED)
       for (int r = tid; r < nown; r += nthr) R.keep((r + 1) * RX);
-    cl.sync();
+    cluster_barrier();
   }
 
   // ---- write the owned active pixels into the buffers current after n iterations --------
@@ -351,7 +393,7 @@ void launch_fused_iteration_cluster(const IterCLArgs& A, bool masked, bool half_
   if (A.n < 1 || A.n > kCLMaxIters) throw ArgError{"cluster-resident iteration: bad iteration count"};
   if (A.P.w <= 0 || A.P.h <= 0) return;
   const CLGeometry g = geometry_of(half_storage, ctas, A.P.w, A.P.h);
-  if (A.rows != g.rows || g.ppt == 0) throw ArgError{"cluster-resident iteration: bad geometry"};
+  if (A.rows != g.rows || A.ctas != ctas || g.ppt == 0) throw ArgError{"cluster-resident iteration: bad geometry"};
   if (masked) {
     if (half_storage) launch_cl_ppt<true, __half>(A, g, ctas, st);
     else launch_cl_ppt<true, float>(A, g, ctas, st);
