@@ -141,8 +141,19 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
   const int rows = A.rows, RX = w + 2, RY = rows + 2, N = ((RX * RY + 3) / 4) * 4;
   const int r0 = rank * rows;                                // first owned row
   const int nown = max(0, min(rows, h - r0));                // owned rows (0 for trailing CTAs)
-  const bool north = rank > 0 && nown > 0;                   // a CTA owns the rows above
-  const bool south = nown == rows && r0 + rows < h;          // a CTA owns the rows below
+  // The halo partners, and the first and last owned rows, are kept in shared memory and read
+  // back (volatile) inside every phase: no flag computed before the cluster barriers is
+  // carried across them in a register.  (Flags held that way were evaluated wrongly on
+  // B200 in some builds of this kernel; the volatile reads keep every evaluation after the
+  // barrier that precedes it.)
+  __shared__ int s_geo[4];  // north rank or -1, south rank or -1, first owned row, last owned row
+  if (threadIdx.x == 0) {
+    s_geo[0] = (rank > 0 && nown > 0) ? rank - 1 : -1;               // a CTA owns the rows above
+    s_geo[1] = (rank + 1 < A.ctas && (rank + 1) * rows < h) ? rank + 1 : -1;  // ... and below
+    s_geo[2] = nown > 0 ? r0 : -1;
+    s_geo[3] = nown > 0 ? r0 + nown - 1 : -1;
+  }
+  const volatile int* geo = s_geo;
   RegionState<ST> R;
   R.carve(smem, N);
   // a halo value goes to the same array element of a neighbour (every CTA has the same layout)
@@ -170,7 +181,6 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
     pi[k] = own ? (ry + 1) * RX + rx + 1 : -1;
     pxy[k] = own ? rx | ((r0 + ry) << 16) : 0;
   }
-  const int last_row = r0 + nown - 1;
   // A cluster barrier, not a CTA barrier: every CTA of the cluster must have started and
   // finished loading its halo rows before a neighbour stores the first iteration's values
   // into them.
@@ -186,10 +196,12 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
       const int i = pi[k];
       if (i < 0) continue;
       const int gx = pxy[k] & 0xffff, gy = pxy[k] >> 16;
-      if (R.template dual<MASKED>(i, RX, gx, gy, w, h, A.sp[j], A.sq[j]) && south && gy == last_row) {
+      const bool wrote = R.template dual<MASKED>(i, RX, gx, gy, w, h, A.sp[j], A.sq[j]);
+      const int south = geo[1];
+      if (wrote && south >= 0 && gy == geo[3]) {
         const int hi = i - nown * RX;  // row 0 of the south CTA's region
-        st_cluster(to(R.tp + hi, rank + 1), R.tp[i]);
-        st_cluster(to(R.q + hi, rank + 1), R.q[i]);
+        st_cluster(to(R.tp + hi, south), R.tp[i]);
+        st_cluster(to(R.q + hi, south), R.q[i]);
       }
     }
     cluster_barrier();
@@ -201,15 +213,16 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
       const int gx = pxy[k] & 0xffff, gy = pxy[k] >> 16;
       if (MASKED && !(R.code[i] & kOn)) R.keep(i);
       else R.template primal<MASKED>(P, i, RX, gx, gy, A.tau[j], A.mu[j]);
-      if (north && gy == r0) {
+      const int north = geo[0], south = geo[1];
+      if (north >= 0 && gy == geo[2]) {
         const int hi = i + rows * RX;  // row rows + 1 of the north CTA's region
-        st_cluster(to(R.ub + hi, rank - 1), R.ub[i]);
-        st_cluster(to(R.v + hi, rank - 1), R.v[i]);
+        st_cluster(to(R.ub + hi, north), R.ub[i]);
+        st_cluster(to(R.v + hi, north), R.v[i]);
       }
-      if (south && gy == last_row) {
+      if (south >= 0 && gy == geo[3]) {
         const int hi = i - nown * RX;
-        st_cluster(to(R.ub + hi, rank + 1), R.ub[i]);
-        st_cluster(to(R.v + hi, rank + 1), R.v[i]);
+        st_cluster(to(R.ub + hi, south), R.ub[i]);
+        st_cluster(to(R.v + hi, south), R.v[i]);
       }
     }
     // column -1 of the owned rows is never written: it alternates like a masked-out pixel
