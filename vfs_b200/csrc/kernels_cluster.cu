@@ -256,6 +256,17 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
 
 namespace {
 
+// Dynamic shared memory a CTA of the kernel may use: the device's opt-in maximum less the
+// kernel's static shared memory (the same for every instantiation).
+int max_dynamic_smem() {
+  int dev = 0, optin = 0;
+  VFS_CUDA(cudaGetDevice(&dev));
+  VFS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  cudaFuncAttributes fa{};
+  VFS_CUDA(cudaFuncGetAttributes(&fa, k_fused_iter_cluster<true, float, 1>));
+  return optin - (int)fa.sharedSizeBytes;
+}
+
 template <bool MASKED, class ST, int PPT>
 void set_cl_attributes() {
   auto k = k_fused_iter_cluster<MASKED, ST, PPT>;
@@ -263,9 +274,7 @@ void set_cl_attributes() {
   int dev = 0;
   VFS_CUDA(cudaGetDevice(&dev));
   if (dev >= 0 && dev < kMaxDevices && configured[dev].load(std::memory_order_acquire)) return;
-  int optin = 0;
-  VFS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  VFS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+  VFS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, max_dynamic_smem()));
   VFS_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
   if (dev >= 0 && dev < kMaxDevices) configured[dev].store(true, std::memory_order_release);
 }
@@ -369,10 +378,8 @@ bool cluster_fits(int variant, bool masked, bool half, int w, int h) {
     if (it != known.end()) return it->second;
   }
   const CLGeometry g = geometry_of(half, ctas, w, h);
-  int optin = 0;
-  VFS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   // (a thread packs a pixel's column and row into one int: 16 bits each)
-  bool ok = g.ppt > 0 && g.bytes <= (size_t)optin && w + 2 <= 4096 && h < 32768;
+  bool ok = g.ppt > 0 && g.bytes <= (size_t)max_dynamic_smem() && w + 2 <= 4096 && h < 32768;
   if (ok) {
     int n = 0;
     if (masked) n = half ? cl_max_clusters_ppt<true, __half>(g, ctas) : cl_max_clusters_ppt<true, float>(g, ctas);
