@@ -190,11 +190,12 @@ int vfs_set_autotune(vfs_stereo* s, int on);
  * 32 x 24, 8: 3 on 23 x 23, 9: 5 on 17 x 17, 12: 7 on 11 x 11, 13: 9 on 5 x 5); 10-11: two
  * horizontally adjacent pixels per thread on 62 x 8 / 62 x 4 tiles; 14-15: the whole level in
  * the shared memory of a thread-block cluster of 16 / 8 CTAs, up to 64 iterations per launch
- * (levels whose state fits: about 3200 pixels per CTA with half storage).  6-15 apply to
- * one-pair launches (other launches, and levels where they do not apply, use variant 1).
+ * (levels whose state fits: about 3200 pixels per CTA with half storage), two cluster
+ * barriers per iteration; 16-17: the same with one cluster barrier per iteration.  6-17 apply
+ * to one-pair launches (other launches, and levels where they do not apply, use variant 1).
  * Every variant gives the same results; this selects speed only.  (No counterpart in the
  * reference.) */
-#define VFS_ITER_VARIANTS 16
+#define VFS_ITER_VARIANTS 18
 int vfs_set_iteration_variant(vfs_stereo* s, int variant);
 /* Force one variant per pyramid level (finest first; levels beyond n_levels use variant 1),
  * e.g. to pin a tuned choice; n_levels = 0 clears it. */

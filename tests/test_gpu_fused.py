@@ -148,7 +148,8 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
     """All variants of the fused iteration kernel (shared-memory tiles of 4 / 8 / 16 rows,
     row-streaming strips of 8 / 16 / 32 rows, 3 to 9 iterations per launch on tiles held in
     shared memory, two pixels per thread on 62-column tiles, the whole level in the shared
-    memory of a 16- or 8-CTA cluster) give the drop-in path's bits
+    memory of a 16- or 8-CTA cluster with two or one cluster barriers per iteration) give the
+    drop-in path's bits
     with float storage and one another's bits with half storage, on sizes that cut tiles
     unevenly.  11 iterations per warp leave a remainder after the multi-iteration launches
     of every K (3, 5, 7, 9).  The 64 x 48 case has no row padding at
@@ -163,7 +164,7 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
         solve_frames(ref, i0, i1, masked, 2)
         want = {n: ref.debug_buffer(n, c) for n, c in (("u", 1), ("u_", 1), ("warpUV", 2), ("Tp", 2))}
         half_ref = None
-        for variant in range(16):
+        for variant in range(18):
             s = make(i0, i1, mask, tv, cv, p, fused=True)
             s.set_iteration_variant(variant)
             solve_frames(s, i0, i1, masked, 2)
@@ -201,7 +202,8 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
 @pytest.mark.parametrize("masked", [True, False])
 @pytest.mark.parametrize("n_iter", [10, 67])
 def test_cluster_resident_iteration_counts(gpu, masked, n_iter):
-    """The cluster-resident variants (14: 16 CTAs, 15: 8 CTAs) with an even number of
+    """The cluster-resident variants (14 / 16: 16 CTAs, 15 / 17: 8 CTAs; two / one cluster
+    barriers per iteration) with an even number of
     iterations per warp (the results stay in the launch's input buffers) and with more
     iterations than one launch takes (64 + 3), over two frames and with CUDA graphs: the
     drop-in path's bits with float storage, variant 1's bits with half storage.  Heights of
@@ -216,7 +218,7 @@ def test_cluster_resident_iteration_counts(gpu, masked, n_iter):
         href.set_iteration_variant(1)
         solve_frames(href, i0, i1, masked, 2)
         hu = href.copy1DDisparityToHost()
-        for variant in (14, 15):
+        for variant in (14, 15, 16, 17):
             s = make(i0, i1, mask, tv, cv, p, fused=True)
             s.set_iteration_variant(variant)
             solve_frames(s, i0, i1, masked, 2)
@@ -264,7 +266,7 @@ def test_per_level_variants_and_tuned_choice_reported(gpu):
     t = make(i0, i1, mask, tv, cv, p, fused=True)
     solve_frames(t, i0, i1, True, 1)  # autotuned
     v = t.iteration_variants()
-    assert len(v) == 3 and all(0 <= x < 16 and not 3 <= x <= 5 for x in v)
+    assert len(v) == 3 and all(0 <= x < 18 and not 3 <= x <= 5 for x in v)
 
 
 @pytest.mark.parametrize("fine,stagger,prio", [(1, 0, 0), (2, 0, 2), (2, 1, 1), (3, 1, 0)])

@@ -281,11 +281,12 @@ inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFT
 // variants 12-13: k_fused_iter_tb with one region pixel per thread, 7 iterations on 11 x 11
 // tiles and 9 on 5 x 5 tiles (for the smallest levels, where the GPU is mostly idle).
 // variants 14-15: k_fused_iter_cluster, the whole level in the shared memory of a cluster of
-// 16 / 8 CTAs, all iterations of a warp (up to kCLMaxIters) per launch; levels that do not
-// fit use the default variant.
-constexpr int kIterVariants = 16;
-constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17, 8, 4, 11, 5, 0, 0};
-constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 3, 6, 0, 0, 0, 0};
+// 16 / 8 CTAs, all iterations of a warp (up to kCLMaxIters) per launch, two cluster
+// barriers per iteration; variants 16-17: k_fused_iter_cluster1, the same with one cluster
+// barrier per iteration.  Levels that do not fit use the default variant.
+constexpr int kIterVariants = 18;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17, 8, 4, 11, 5, 0, 0, 0, 0};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 3, 6, 0, 0, 0, 0, 0, 0};
 constexpr int kIterFirstRowsVariant = 3;
 constexpr int kIterFirstTBVariant = 6;
 constexpr int kIterFirstX2Variant = 10;
