@@ -149,8 +149,12 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
     c = P.c[pos];
   }
   // masked form: a block with no pixel on in its region writes nothing and reads nothing
-  // another block needs, so it leaves here
-  if (MASKED && !__syncthreads_or(in_img && (code & kOn))) return;
+  // another block needs, so it leaves here.  With tile spans the grid holds only tiles
+  // between a row's first and last tile with a pixel on, which for the fisheye circle all
+  // have one; there the block-wide vote would only make every warp wait for the first load
+  // round before any issues the second, so it is skipped (a tile without a pixel on then
+  // does its few loads and writes nothing, as before).
+  if (MASKED && A.span_rows == 0 && !__syncthreads_or(in_img && (code & kOn))) return;
   if (in_img) {
     bool own = F::dual_at(P, pin, qin, ix, iy, pos, code, a, b, c, A.sp[pi_], A.sq[pi_], ubar, vb, pp, qq, tp, tile,
                           u_th, Iu_th, Iz_th);
