@@ -32,6 +32,10 @@
 // When the level has no row padding (stride == width), column -1 of a row is the previous
 // row's last pixel, which changes every iteration; the caller then uses this kernel only if
 // no pixel of column 0 is on (StereoTgvImpl::tb_ok), as for the temporally blocked form.
+//
+// k_fused_iter_cluster1 below is the same solve with one cluster barrier per iteration
+// (variants 16-17).  On B200 it measured slower than the two-barrier form, and it is kept
+// as a forced variant.
 #include "common.cuh"
 #include "fused.cuh"
 #include "region_step.cuh"
@@ -51,7 +55,7 @@ constexpr int kCLMaxPixelsPerThread = 3;
 
 struct CLGeometry {
   int rows = 0;         // image rows per CTA
-  int rx = 0, ry = 0;   // region columns (w + 2) and rows (rows + 2)
+  int rx = 0, ry = 0;   // region columns (w + 2) and rows (rows + 2; rows + 3 for the one-barrier form)
   int n = 0;            // elements per array (a multiple of 4)
   size_t bytes = 0;     // dynamic shared memory per CTA
   int ppt = 0;          // owned pixels per thread (1 .. kCLMaxPixelsPerThread)
