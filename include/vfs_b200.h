@@ -213,18 +213,19 @@ int vfs_batch_set_iteration_variant(vfs_batch* b, int variant);
 int vfs_equalize_hist_u8(const uint8_t* d_src, uint8_t* d_dst, size_t n, void* cuda_stream);
 
 /* Histogram equalisation that allocates nothing (no counterpart in the reference).
- * For callers that cannot allocate device memory at the point of the call: code recorded
- * into a CUDA graph or running inside a stream capture, where an allocation would become
- * part of the capture or be refused; real-time camera threads, where cudaMalloc / cudaFree
- * can stall on device-wide synchronisation; and hosts whose device memory is already
- * reserved by another allocator.  It equalises `count` images of n pixels each, stored back
- * to back at d_src (results at d_dst, which may equal d_src), like vfs_equalize_hist_u8.
+ * For callers that cannot allocate device memory where they call it: real-time camera
+ * threads with a latency budget, where cudaMalloc / cudaFree can synchronise the whole device
+ * and stall for an unbounded time; and hosts that hand all of the GPU's memory to their own
+ * allocator or pool up front, so that a library allocation would fail or break the budget.
+ * It equalises `count` images of n pixels each, stored back to back at d_src (results at
+ * d_dst, which may equal d_src), like vfs_equalize_hist_u8.
  * Limits: count <= VFS_NOALLOC_MAX_IMAGES (16) and n <= 2^32 - 1; larger requests return
  * VFS_ERR_ARG with a message in vfs_last_error(NULL).  The scratch is a 20 KiB array that
- * each GPU loading the library keeps until exit, shared by every call on that GPU: calls
- * whose work overlaps on the GPU (different streams, or host threads without ordering)
- * race on it, so order them on one stream.  The first call on a device resolves the
- * array's device address; make that first call before any stream capture. */
+ * each GPU loading the library keeps until exit, shared by every call on that GPU; each call
+ * clears the histograms it uses.  Calls whose work overlaps on the GPU (different streams,
+ * or host threads without ordering) race on the array, so order them on one stream.
+ * The first call on a device (and the first after cudaDeviceReset or under another CUDA
+ * context) looks up the array's device address with cudaGetSymbolAddress and caches it. */
 #define VFS_NOALLOC_MAX_IMAGES 16
 int vfs_equalize_hist_u8_noalloc(const uint8_t* d_src, uint8_t* d_dst, size_t n, int count,
                                  void* cuda_stream);

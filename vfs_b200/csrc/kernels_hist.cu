@@ -61,8 +61,9 @@ __global__ void k_equalize_lut(const unsigned int* __restrict__ hist, size_t tot
   }
 }
 
-__global__ void k_apply_lut(const uint8_t* __restrict__ src, uint8_t* __restrict__ dst, size_t n,
-                            const uint8_t* __restrict__ lut) {
+// src and dst may be the same buffer (in-place equalisation): each thread reads its element
+// before writing it, and the pointers are deliberately not __restrict__.
+__global__ void k_apply_lut(const uint8_t* src, uint8_t* dst, size_t n, const uint8_t* __restrict__ lut) {
   __shared__ uint8_t sl[256];
   for (int i = threadIdx.x; i < 256; i += blockDim.x) sl[i] = lut[i];
   __syncthreads();
@@ -93,8 +94,10 @@ void launch_equalize_hist(const uint8_t* src, uint8_t* dst, size_t n, unsigned i
 // Its scratch -- one 256-bin histogram and one 256-byte LUT per image -- lives in this
 // file-scope device array, which every GPU that loads the library holds until the process
 // exits.  Host code cannot use the array's name as a device address (on the host it is
-// only a stand-in), so the first call on each device resolves the address with
-// cudaGetSymbolAddress while that device is current and keeps it for later calls.
+// only a stand-in), so the address is resolved with cudaGetSymbolAddress while the device is
+// current and cached.  The cache is keyed by the device AND the id of its current CUDA
+// context: after cudaDeviceReset (or under another context) the module is loaded again at a
+// new address, so a changed context id makes the next call resolve the address afresh.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr size_t kSlotBytes = 256 * sizeof(unsigned int) + 256;  // histogram + LUT of one image
@@ -102,7 +105,41 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[VFS_NOALLOC_MAX
 
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
-void* g_noalloc_addr[kMaxDevices] = {};
+struct NoallocAddr {
+  unsigned long long ctx_id = 0;  // context the address belongs to (0 = none yet)
+  void* addr = nullptr;
+};
+NoallocAddr g_noalloc_addr[kMaxDevices];
+
+// cuCtxGetCurrent / cuCtxGetId, reached through the runtime's driver entry points (the library
+// does not link libcuda directly).
+typedef int (*PfnCtxGetCurrent)(void** ctx);
+typedef int (*PfnCtxGetId)(void* ctx, unsigned long long* id);
+PfnCtxGetCurrent g_ctx_get_current = nullptr;
+PfnCtxGetId g_ctx_get_id = nullptr;
+std::once_flag g_ctx_fns_once;
+
+// Id of the calling thread's current context (unique for the life of the process), or 0.
+unsigned long long current_context_id() {
+  std::call_once(g_ctx_fns_once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = (PfnCtxGetCurrent)f;
+    f = nullptr;
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_id = (PfnCtxGetId)f;
+    (void)cudaGetLastError();
+  });
+  if (!g_ctx_get_current || !g_ctx_get_id) return 0;
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (g_ctx_get_current(&ctx) != 0 || !ctx) return 0;
+  if (g_ctx_get_id(ctx, &id) != 0) return 0;
+  return id;
+}
 }  // namespace
 
 namespace vfs {
@@ -130,20 +167,35 @@ extern "C" int vfs_equalize_hist_u8_noalloc(const uint8_t* d_src, uint8_t* d_dst
     vfs::set_global_error("vfs_equalize_hist_u8_noalloc: no usable current device");
     return VFS_ERR_CUDA;
   }
+  unsigned long long ctx = current_context_id();
+  if (ctx == 0) {
+    // No context is current on this thread yet: cudaSetDevice makes the device's primary
+    // context current (the one the kernels below will run in).
+    if (cudaSetDevice(dev) != cudaSuccess) {
+      (void)cudaGetLastError();
+      vfs::set_global_error("vfs_equalize_hist_u8_noalloc: no usable current device");
+      return VFS_ERR_CUDA;
+    }
+    ctx = current_context_id();
+  }
   unsigned char* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
+    NoallocAddr& slot = g_noalloc_addr[dev];
+    // Without a context id (driver entry points unavailable) the address is resolved on every call.
+    if (!slot.addr || ctx == 0 || slot.ctx_id != ctx) {
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
       if (e != cudaSuccess || !p) {
         (void)cudaGetLastError();
+        slot = NoallocAddr{};
         vfs::set_global_error("vfs_equalize_hist_u8_noalloc: cudaGetSymbolAddress failed");
         return VFS_ERR_CUDA;
       }
-      g_noalloc_addr[dev] = p;
+      slot.addr = p;
+      slot.ctx_id = ctx;
     }
-    scratch = (unsigned char*)g_noalloc_addr[dev];
+    scratch = (unsigned char*)slot.addr;
   }
   cudaStream_t st = (cudaStream_t)cuda_stream;
   try {
