@@ -58,6 +58,16 @@ int vfs_initialize(vfs_stereo* s, int width, int height, float beta, float gamma
  * baseline / focal (stereotgv.h:31-32, set by dllhook/vfs.cpp:15-16). */
 int vfs_set_limit_range(vfs_stereo* s, float limit_range);
 int vfs_set_camera(vfs_stereo* s, float baseline, float focal);
+
+/* Arithmetic of the diffusion-tensor weight exp(-beta |grad I|^gamma) (no counterpart in the
+ * reference, which always calls CUDA's expf / powf there: calcTensor.cu:60-64).
+ * VFS_TENSOR_MATH_CUDA (the default) makes the same calls, so a solve reproduces the
+ * reference's CUDA build.  VFS_TENSOR_MATH_PORTABLE uses an exp / log built only from
+ * correctly rounded IEEE operations, which a CPU restatement reproduces bit for bit; the two
+ * weights agree to 1.5e-6 relative.  Applies to both solve paths from the next solve on. */
+#define VFS_TENSOR_MATH_CUDA 0
+#define VFS_TENSOR_MATH_PORTABLE 1
+int vfs_set_tensor_math(vfs_stereo* s, int mode);
 /* Pyramid geometry of an initialized handle: level sizes and pitches (elements). */
 int vfs_get_level_size(const vfs_stereo* s, int level, int* width, int* height, int* stride);
 

@@ -26,9 +26,10 @@ struct Ref {
     StereoTgv s;
     bool initialized = false;
     // Set by vref_copy_mask when some pyramid level of the mask has an on pixel in its first or
-    // last row or column.  The reference's masked kernels then form neighbour indices outside
-    // their buffers (thresholdingL1.cu:139-177, updateDualVariables.cu: the `up` index of row 0
-    // is negative), so a masked solve is refused instead of run.
+    // last row or column.  The reference's masked kernels then form neighbour indices before
+    // their buffers' start (thresholdingL1.cu:139-177: the `up` index of row 0 is negative);
+    // in this build those reads land in the zero guard of every allocation
+    // (refcompat/vfs_ref_compat.h) and read 0.
     bool mask_touches_border = false;
     int border_level = -1;
 };
@@ -97,7 +98,7 @@ void vref_destroy(void* h) {
                       s->d_cv, s->d_i1calibrated, s->d_X, s->debug_depth};
     cudaDeviceSynchronize();
     for (void* p : fields) add(p);
-    for (void* p : ptrs) cudaFree(p);
+    for (void* p : ptrs) vfs_ref_cuda_free(p);
     delete r;
 }
 
@@ -112,6 +113,11 @@ int vref_initialize(void* h, int w, int hgt, float beta, float gamma, float alph
         // The tensor kernels size their x grid from the height (calcTensor.cu:81,227); with
         // height > width their threads index past the last row.
         g_err = "height > width is not supported by the reference build";
+        return -1;
+    }
+    if ((size_t((w + 31) / 32 * 32) + 1) * 16 > kVfsRefGuard) {
+        // reads before a buffer's start reach back one row of float4 at most
+        g_err = "width too large for the allocation guard of the reference build";
         return -1;
     }
     StereoTgv* s = &r->s;
@@ -163,7 +169,7 @@ int vref_copy_mask(void* h, const float* mask) {
     });
 }
 
-// 1 when the current mask reaches an image border at some level (masked solves are refused).
+// 1 when the current mask reaches an image border at some pyramid level.
 int vref_mask_touches_border(void* h) { return static_cast<Ref*>(h)->mask_touches_border ? 1 : 0; }
 
 int vref_copy_images_u8(void* h, const uint8_t* i0, const uint8_t* i1) {
@@ -185,11 +191,6 @@ int vref_copy_images_mat(void* h, const void* i0, const void* i1, int kind) {
 int vref_solve(void* h, int masked) {
     Ref* r = static_cast<Ref*>(h);
     StereoTgv* s = &r->s;
-    if (masked && r->mask_touches_border) {
-        g_err = "mask has on pixels on the border of pyramid level " + std::to_string(r->border_level) +
-                ": the reference's masked kernels would read outside their buffers";
-        return -1;
-    }
     if (s->width < 2 || s->height < 2) {
         g_err = "images must be at least 2 x 2";
         return -1;

@@ -20,6 +20,11 @@
 //  * cudaMalloc.  The reference leaves its buffers uninitialised, and masked-out pixels carry
 //    whatever a buffer held (stale-value behaviour).  Every allocation is zero-filled here so
 //    that runs are deterministic and comparable with implementations that start from zero.
+//    Each allocation also gets a zero-filled guard zone of kVfsRefGuard bytes before and after
+//    it: where the mask reaches the first image row, the masked kernels form neighbour indices
+//    up to one row before the buffer start (e.g. the `up` index of row 0 in
+//    thresholdingL1.cu:139-177), which on the reference's own build reads whatever memory lies
+//    there.  Here such reads land in the guard and read 0.  Release with vfs_ref_cuda_free.
 //  * helper_cuda.h (CUDA Samples) and OpenCV: see helper_cuda.h and opencv2/opencv.hpp beside
 //    this file.  checkCudaErrors throws instead of calling exit(), so that a failure surfaces
 //    as an error code at the C wrapper (oracle/ref_capi.cu) rather than ending the process.
@@ -92,9 +97,22 @@ inline cudaError_t cudaBindTexture2D(size_t* offset, vfs_ref_texture<T, Dim, Mod
 #define texture __managed__ vfs_ref_texture
 
 // ---------------------------------------------------------------- zero-filled allocations
+constexpr size_t kVfsRefGuard = 64 * 1024;  // > one row of float4 at any supported width
+
 inline cudaError_t vfs_ref_cuda_malloc_zero(void** p, size_t n) {
-    cudaError_t e = cudaMalloc(p, n);
+    void* base = nullptr;
+    cudaError_t e = cudaMalloc(&base, n + 2 * kVfsRefGuard);
     if (e != cudaSuccess) return e;
-    return cudaMemset(*p, 0, n);
+    e = cudaMemset(base, 0, n + 2 * kVfsRefGuard);
+    if (e != cudaSuccess) {
+        cudaFree(base);
+        return e;
+    }
+    *p = static_cast<char*>(base) + kVfsRefGuard;
+    return cudaSuccess;
+}
+
+inline cudaError_t vfs_ref_cuda_free(void* p) {
+    return p ? cudaFree(static_cast<char*>(p) - kVfsRefGuard) : cudaSuccess;
 }
 #define cudaMalloc(p, n) vfs_ref_cuda_malloc_zero(reinterpret_cast<void**>(p), (n))

@@ -26,10 +26,14 @@ def params(beta=10.0, gamma=0.8, alpha0=17.0, alpha1=1.2, tsl=1.0, lam=5.0, n_le
                 f_scale=f_scale, n_warp=n_warp, n_iter=n_iter, limit_range=limit_range)
 
 
-def run_gpu(i0, i1, mask, tv, cv, p, masked=True, frames=1, solver=None):
+def run_gpu(i0, i1, mask, tv, cv, p, masked=True, frames=1, solver=None, portable=False):
+    """The drop-in solve through the C ABI.  portable=True computes the tensor weight with the
+    portable exp / log that the CPU oracle restates bit for bit (the comparisons with the
+    oracle use it); the default calls CUDA's expf / powf as the reference does."""
     from vfs_b200.stereotgv import StereoTgv
     h, w = i0.shape[:2]
     s = solver or StereoTgv()
+    s.set_tensor_math(portable)
     s.limitRange = p["limit_range"]
     s.initialize(w, h, p["beta"], p["gamma"], p["alpha0"], p["alpha1"], p["tsl"], p["lam"], p["n_levels"],
                  p["f_scale"], p["n_warp"], p["n_iter"])

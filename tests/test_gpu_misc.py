@@ -101,7 +101,7 @@ def test_image_overloads(gpu, kind):
         f = lambda x: ((x[..., 0].astype(np.float32) + x[..., 1].astype(np.float32) + x[..., 2].astype(np.float32))
                        / np.float32(3)) / np.float32(256)
         oa, ob = f(a), f(b)
-    s = run_gpu(a, b, mask, tv, cv, p, True)
+    s = run_gpu(a, b, mask, tv, cv, p, True, portable=True)
     o = run_oracle(oa, ob, mask, tv, cv, p, True, precision=32)
     assert diff_stats(s.copy1DDisparityToHost(), o.get("u"))["max"] <= 1e-6
 
@@ -110,7 +110,7 @@ def test_convert_kb_and_colour_map(gpu):
     d = np.load(os.path.join(os.path.dirname(__file__), "golden", "wang_half", "wang_half.npz"))
     mask = d["mask_u8"].astype(np.float32) / 255.0
     p = params(beta=9.0, gamma=0.85, n_levels=3, n_warp=2, n_iter=5, limit_range=0.1)
-    s = run_gpu(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True)
+    s = run_gpu(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True, portable=True)
     o = run_oracle(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True, precision=32)
     kb = (143.259, 143.301, 211.571, 196.661, -0.00727452, 0.05200624, -0.0510574, 0.01108238, -0.0639505,
           0.000184912, -0.0000766807)

@@ -25,7 +25,7 @@ def test_small_random_cases(gpu, masked, size):
     w, h = size
     i0, i1, mask, tv, cv = random_case(w, h, seed=w * 7 + h)
     p = params(n_levels=2, n_warp=2, n_iter=7)
-    s = run_gpu(i0, i1, mask, tv, cv, p, masked)
+    s = run_gpu(i0, i1, mask, tv, cv, p, masked, portable=True)
     o = run_oracle(i0, i1, mask, tv, cv, p, masked, precision=32)
     for name, comps in (("u", 1), ("warpUV", 2), ("u_", 1)):
         st = diff_stats(s.debug_buffer(name, comps), o.get(name, comps))
@@ -36,7 +36,7 @@ def test_single_level_intermediates(gpu):
     # one level, one warp, one iteration: every intermediate is a single kernel deep
     i0, i1, mask, tv, cv = random_case(80, 61, seed=3)
     p = params(n_levels=1, n_warp=1, n_iter=1)
-    s = run_gpu(i0, i1, mask, tv, cv, p, True)
+    s = run_gpu(i0, i1, mask, tv, cv, p, True, portable=True)
     o = run_oracle(i0, i1, mask, tv, cv, p, True, precision=32)
     for name, comps, tol in (("i1warp", 1, 0), ("Iz", 1, 0), ("Iu", 1, 1e-7), ("i0smooth", 1, 0),
                              ("a", 1, 1e-6), ("b", 1, 1e-6), ("c", 1, 1e-6), ("etau", 1, 1e-5),
@@ -49,7 +49,7 @@ def test_state_persists_across_frames(gpu):
     # the reference keeps stale values in masked-out pixels between frames
     i0, i1, mask, tv, cv = random_case(72, 60, seed=11)
     p = params(n_levels=2, n_warp=2, n_iter=4)
-    s = run_gpu(i0, i1, mask, tv, cv, p, True, frames=3)
+    s = run_gpu(i0, i1, mask, tv, cv, p, True, frames=3, portable=True)
     o = run_oracle(i0, i1, mask, tv, cv, p, True, precision=32, frames=3)
     st = diff_stats(s.copy1DDisparityToHost(), o.get("u"))
     assert st["max"] <= TOL_MAX_F32, st
@@ -59,7 +59,7 @@ def test_wang_golden_config(gpu):
     d = np.load(os.path.join(os.path.dirname(__file__), "golden", "wang_half", "wang_half.npz"))
     p = params(beta=9.0, gamma=0.85, n_levels=5, n_warp=20, n_iter=10, limit_range=0.1)
     mask = d["mask_u8"].astype(np.float32) / 255.0
-    s = run_gpu(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True)
+    s = run_gpu(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True, portable=True)
     o32 = run_oracle(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True, precision=32)
     m = mask > 0
     u = s.copy1DDisparityToHost()
@@ -77,7 +77,7 @@ def test_synthetic_benchmark_configs(gpu, wh):
     sp = synth.SOLVER_PARAMS
     p = params(beta=sp["beta"], gamma=sp["gamma"], n_levels=synth.n_levels_for(w), n_warp=sp["nWarpIters"],
                n_iter=sp["nSolverIters"], limit_range=synth.LIMIT_RANGE)
-    s = run_gpu(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True)
+    s = run_gpu(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True, portable=True)
     u = s.copy1DDisparityToHost()
     m = pair.mask > 0
     o32 = run_oracle(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True, precision=32)

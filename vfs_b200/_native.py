@@ -44,6 +44,7 @@ SIGNATURES = {
     "vfs_initialize": [_vp, _i, _i, _f, _f, _f, _f, _f, _f, _i, _f, _i, _i],
     "vfs_set_limit_range": [_vp, _f],
     "vfs_set_camera": [_vp, _f, _f],
+    "vfs_set_tensor_math": [_vp, _i],
     "vfs_get_level_size": [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)],
     "vfs_load_vector_fields": [_vp, _vp, _vp],
     "vfs_copy_mask_to_device": [_vp, _vp],

@@ -120,6 +120,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         d.xmax = std::min(d.w, xcov);
         d.beta = s->P.beta;
         d.gamma = s->P.gamma;
+        d.cuda_math = s->tensor_cuda_math;
         set_tiles(L, k, d.w, d.h);
       }
       L.npairs = na;

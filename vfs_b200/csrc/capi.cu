@@ -164,7 +164,20 @@ int vfs_initialize(vfs_stereo* s, int width, int height, float beta, float gamma
 }
 
 int vfs_set_limit_range(vfs_stereo* s, float lr) {
-  return guarded(s, [&] { s->impl.P.limitRange = lr; });
+  return guarded(s, [&] {
+    if (s->impl.P.limitRange != lr) s->impl.generation = vfs::next_generation();  // captured graphs hold it
+    s->impl.P.limitRange = lr;
+  });
+}
+
+int vfs_set_tensor_math(vfs_stereo* s, int mode) {
+  return guarded(s, [&] {
+    if (mode != VFS_TENSOR_MATH_CUDA && mode != VFS_TENSOR_MATH_PORTABLE)
+      throw vfs::ArgError{"vfs_set_tensor_math: mode must be VFS_TENSOR_MATH_CUDA or VFS_TENSOR_MATH_PORTABLE"};
+    const int cuda_math = mode == VFS_TENSOR_MATH_CUDA ? 1 : 0;
+    if (s->impl.tensor_cuda_math != cuda_math) s->impl.generation = vfs::next_generation();
+    s->impl.tensor_cuda_math = cuda_math;
+  });
 }
 
 int vfs_set_camera(vfs_stereo* s, float baseline, float focal) {

@@ -226,6 +226,7 @@ struct LevelPair {
   int init_flow;         // 1 at a pair's coarsest level
   int w, h, s, xmax, tiles_x, tile0;
   float beta, gamma;
+  int cuda_math;  // tensor weight from CUDA's expf / powf (1) or the portable construction (0)
 };
 struct LevelArgs {
   int npairs, ntiles;

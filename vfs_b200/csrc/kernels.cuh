@@ -35,8 +35,10 @@ void launch_derivatives_fisheye(cudaTextureObject_t i0, cudaTextureObject_t i1w,
 // calcTensor.cu:99-128 (mask == nullptr) and :245-273
 void launch_gaussian(cudaTextureObject_t in, const float* mask, float* out, Geom g, cudaStream_t st);
 // calcTensor.cu:8-73 / :155-219; columns >= xmax are not computed
+// cuda_math: tensor weight from CUDA's expf / powf (1, as the reference) or the portable
+// construction of tgv_math.cuh (0)
 void launch_calc_tensor(cudaTextureObject_t gray, const float* mask, float beta, float gamma, float* a, float* b,
-                        float* c, Geom g, int xmax, cudaStream_t st);
+                        float* c, Geom g, int xmax, int cuda_math, cudaStream_t st);
 // preconditioning.cu:3-22 / :41-60
 void launch_solve_eta(const float* mask, float alpha0, float alpha1, const float* a, const float* b,
                       const float* c, float* etau, float* etav1, float* etav2, Geom g, cudaStream_t st);

@@ -476,7 +476,7 @@ __global__ void __launch_bounds__(kFTW* kFTH) k_level_tensor(const __grid_consta
     ny = 0.0f;
   }
   float ntx = ny, nty = -nx;
-  float wt = tgv_exp(-P.beta * tgv_pow(abs_img, P.gamma));
+  float wt = tensor_weight(abs_img, P.beta, P.gamma, P.cuda_math);
   if (!(wt > 1e-8f)) wt = 1e-8f;
   P.a[pos] = wt * nx * nx + ntx * ntx;
   P.c[pos] = wt * nx * ny + ntx * nty;

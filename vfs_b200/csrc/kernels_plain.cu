@@ -168,7 +168,7 @@ __global__ void k_gaussian(cudaTextureObject_t in, const float* __restrict__ mas
 }
 
 __global__ void k_calc_tensor(cudaTextureObject_t gray, const float* __restrict__ mask, float beta, float gamma,
-                              float* A, float* B, float* C, Geom g, int xmax) {
+                              float* A, float* B, float* C, Geom g, int xmax, int cuda_math) {
   int ix, iy;
   if (!pixel(ix, iy, xmax, g.h)) return;
   int pos = ix + iy * g.s;
@@ -186,9 +186,7 @@ __global__ void k_calc_tensor(cudaTextureObject_t gray, const float* __restrict_
     ny = 0.0f;
   }
   float ntx = ny, nty = -nx;
-  // calcTensor.cu:61-64 uses expf / powf; tgv_exp / tgv_pow give the same values to a few
-  // ulp with bits that a host restatement reproduces exactly.
-  float wt = tgv_exp(-beta * tgv_pow(abs_img, gamma));
+  float wt = tensor_weight(abs_img, beta, gamma, cuda_math);
   if (!(wt > 1e-8f)) wt = 1e-8f;
   A[pos] = wt * nx * nx + ntx * ntx;
   C[pos] = wt * nx * ny + ntx * nty;
@@ -526,9 +524,9 @@ void launch_gaussian(cudaTextureObject_t in, const float* mask, float* out, Geom
   VFS_LAUNCH_CHECK();
 }
 void launch_calc_tensor(cudaTextureObject_t gray, const float* mask, float beta, float gamma, float* a, float* b,
-                        float* c, Geom g, int xmax, cudaStream_t st) {
+                        float* c, Geom g, int xmax, int cuda_math, cudaStream_t st) {
   if (xmax <= 0) return;
-  k_calc_tensor<<<grid2d(xmax, g.h), block2d(), 0, st>>>(gray, mask, beta, gamma, a, b, c, g, xmax);
+  k_calc_tensor<<<grid2d(xmax, g.h), block2d(), 0, st>>>(gray, mask, beta, gamma, a, b, c, g, xmax, cuda_math);
   VFS_LAUNCH_CHECK();
 }
 void launch_solve_eta(const float* mask, float alpha0, float alpha1, const float* a, const float* b, const float* c,

@@ -394,7 +394,8 @@ void StereoTgvImpl::solveReference(bool masked) {
     if (level == P.nLevels - 1) launch_optical_flow_vector(d_u, pTvF[level], d_warpUV, g, st);
     launch_gaussian(t1(pI0[level], level), mk, d_i0smooth, g, st);
     int xcov = ((g.h + blockWidth - 1) / blockWidth) * blockWidth;  // calcTensor.cu:81,227
-    launch_calc_tensor(t1(d_i0smooth, level), mk, P.beta, P.gamma, d_a, d_b, d_c, g, std::min(g.w, xcov), st);
+    launch_calc_tensor(t1(d_i0smooth, level), mk, P.beta, P.gamma, d_a, d_b, d_c, g, std::min(g.w, xcov),
+                       tensor_cuda_math, st);
     launch_solve_eta(mk, P.alpha0, P.alpha1, d_a, d_b, d_c, d_etau, d_etav1, d_etav2, g, st);
     for (int warpIter = 0; warpIter < P.nWarpIters; warpIter++) {
       VFS_CUDA(cudaMemsetAsync(d_p, 0, 2 * f, st));

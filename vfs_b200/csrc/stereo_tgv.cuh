@@ -107,6 +107,9 @@ class StereoTgvImpl {
 
   SolverParams P;
   float baseline = 0.0f, focal = 0.0f;
+  // tensor weight from CUDA's expf / powf as the reference (1, default) or from the portable
+  // exp / log of tgv_math.cuh that the CPU oracle restates bit for bit (0)
+  int tensor_cuda_math = 1;
   bool visualizeResults = false;
   int blockWidth, blockHeight, strideAlignment;
   int width = 0, height = 0, stride = 0;

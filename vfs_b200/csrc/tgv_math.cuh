@@ -83,4 +83,15 @@ TGV_HD float tgv_pow(float a, float g) {
   return tgv_fma(t, err, t);      // e^(y + err) ~ e^y (1 + err)
 }
 
+#ifdef __CUDACC__
+// Diffusion-tensor weight exp(-beta |grad I|^gamma) before its 1e-8 floor (calcTensor.cu:60-64).
+// cuda_math != 0: CUDA's expf / powf, the calls the reference makes, so the tensor is the
+// reference's to the bit (the default).  cuda_math == 0: the portable construction above,
+// which a host restatement reproduces bit for bit.
+__device__ __forceinline__ float tensor_weight(float abs_img, float beta, float gamma, int cuda_math) {
+  if (cuda_math) return expf(-beta * powf(abs_img, gamma));
+  return tgv_exp(-beta * tgv_pow(abs_img, gamma));
+}
+#endif
+
 }  // namespace vfs

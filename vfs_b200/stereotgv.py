@@ -71,6 +71,11 @@ class StereoTgv:
         self._limit_range = float(v)
         check(self._h, self._L.vfs_set_limit_range(self._h, self._limit_range))
 
+    def set_tensor_math(self, portable: bool) -> None:
+        """Tensor weight from CUDA's expf / powf as the reference (False, the default) or from
+        the portable exp / log that the CPU oracle restates bit for bit (True)."""
+        check(self._h, self._L.vfs_set_tensor_math(self._h, 1 if portable else 0))
+
     def set_stream(self, stream) -> None:
         """Run on a torch.cuda.Stream (or a raw cudaStream_t integer)."""
         raw = getattr(stream, "cuda_stream", stream)
