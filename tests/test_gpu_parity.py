@@ -1,10 +1,15 @@
 """CUDA drop-in path (through the C ABI) against the CPU oracle on the same inputs.
 
-Tolerances: the float32 oracle restates the reference kernels with the same operation
-order as the CUDA kernels, so the two agree to float32 rounding of the few library
-functions (expf, powf) and of rare texture-filter ties: max |du| <= 1e-3 px (the drop-in
-bar).  Against the float64 oracle (the method in double precision) the mean disparity
-error must stay <= 0.05 px.
+The GPU solves here compute the tensor weight with the portable exp / log (vfs_set_tensor_math)
+that the float32 oracle restates bit for bit, so the two evaluate the same float operations in
+the same order.  What remains is the texture unit: the oracle models its filtering from samples
+recorded on B200 (exact on 99.98 % of them, 1 ulp off on the rest), and a 1-ulp sample, fed back
+through 150 iterations per level and the warping, can move a pixel's disparity by a few 1e-3 px.
+Bars: max |du| <= 1e-3 px on the small cases, the masked benchmark configurations and the Wang
+configuration; for the unmasked benchmark configurations mean <= 1e-4 px and at most 0.1 % of
+pixels beyond 1e-3 px.  The max-abs bar against the reference itself, at every size, is carried
+by tests/test_gpu_ref_build.py (bit-identical to the reference's own CUDA build).  Against the
+float64 oracle (the method in double precision) the mean disparity error must stay <= 0.05 px.
 """
 import os
 
@@ -63,25 +68,29 @@ def test_wang_golden_config(gpu):
     o32 = run_oracle(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True, precision=32)
     m = mask > 0
     u = s.copy1DDisparityToHost()
-    st = diff_stats(u, o32.get("u"), m)
-    assert st["mean"] <= 1e-4, st
+    st = diff_stats(u, o32.get("u"))
+    assert st["max"] <= TOL_MAX_F32 and st["mean"] <= 1e-6, st
     o64 = run_oracle(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True, precision=64)
     assert diff_stats(u, o64.get("u"), m)["mean"] <= TOL_MEAN_F64
 
 
+@pytest.mark.parametrize("masked", [True, False], ids=["masked", "plain"])
 @pytest.mark.parametrize("wh", [(424, 400), (848, 800)])
-def test_synthetic_benchmark_configs(gpu, wh):
+def test_synthetic_benchmark_configs(gpu, wh, masked):
     from vfs_b200 import synth
     w, h = wh
     pair = synth.make_pair(w, h, seed=1000 + w)
     sp = synth.SOLVER_PARAMS
     p = params(beta=sp["beta"], gamma=sp["gamma"], n_levels=synth.n_levels_for(w), n_warp=sp["nWarpIters"],
                n_iter=sp["nSolverIters"], limit_range=synth.LIMIT_RANGE)
-    s = run_gpu(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True, portable=True)
+    s = run_gpu(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, masked, portable=True)
     u = s.copy1DDisparityToHost()
+    o32 = run_oracle(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, masked, precision=32)
+    d = np.abs(u.astype(np.float64) - o32.get("u"))
+    if masked:
+        assert d.max() <= TOL_MAX_F32, d.max()
+    else:
+        assert d.mean() <= 1e-4 and (d > TOL_MAX_F32).mean() <= 1e-3, (d.mean(), (d > TOL_MAX_F32).sum())
     m = pair.mask > 0
-    o32 = run_oracle(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True, precision=32)
-    st = diff_stats(u, o32.get("u"), m)
-    assert st["mean"] <= 1e-4 and st["p99"] <= TOL_MAX_F32, st
-    o64 = run_oracle(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, True, precision=64)
+    o64 = run_oracle(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, masked, precision=64)
     assert diff_stats(u, o64.get("u"), m)["mean"] <= TOL_MEAN_F64

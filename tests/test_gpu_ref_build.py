@@ -5,15 +5,16 @@ oracle/refcompat/ for the texture-reference API CUDA 12 removed, helper_cuda.h a
 OpenCV calls) into oracle/_ref/.  These tests run that build and the vfs_b200 drop-in path on
 the same inputs and compare their outputs.
 
-Two builds of the reference are compared:
-* ``nofma``: compiled with -fmad=false, the contraction rule of the vfs_b200 library.  The two
-  then evaluate the same float operations in the same order, and the only arithmetic that
-  differs is the tensor weight exp(-beta |grad I|^gamma), where the reference calls CUDA's
-  expf / powf and vfs_b200 uses its own exp / log construction.  Bar: max |du| <= 1e-3 px.
-* ``stock``: nvcc's default flags, multiply-add contraction on, as the reference ships.  Every
-  a*b+c the compiler contracts rounds once instead of twice, so this build differs from the
-  ``nofma`` build of the same sources by float32 rounding that 150 iterations per level
-  amplify.
+Two builds of the reference are used:
+* ``nofma``: compiled with -fmad=false, the contraction rule of the vfs_b200 library.  The
+  drop-in path (tensor weight through CUDA's expf / powf, its default) evaluates the same float
+  operations in the same order through the same texture unit, and its results are required to
+  be BIT-IDENTICAL to this build's: every plane, at every size, masked and plain.
+* ``stock``: nvcc's default flags (multiply-add contraction on), as the reference ships.  Every
+  a*b+c the compiler contracts rounds once instead of twice; over 150 iterations per level that
+  changes the reference's own result (by up to 0.1 px at 848x800 and 0.5 px on the Wang case).
+  No float32 reimplementation can be closer to it than its own -fmad=false build is, so the
+  tests hold the drop-in path to exactly that distance.
 
 The CPU float32 oracle (oracle/tgv_oracle.cpp) is pinned to the reference build here as well.
 """
@@ -37,50 +38,67 @@ def ref():
     return R
 
 
-@pytest.mark.parametrize("fma", [False, True], ids=["nofma", "stock"])
+def _exact(got, want, what):
+    st = diff_stats(got, want)
+    assert st["max"] == 0.0, (what, st)
+
+
 @pytest.mark.parametrize("masked", [True, False], ids=["masked", "plain"])
 @pytest.mark.parametrize("size", [(67, 53), (96, 64), (130, 101)])
-def test_small_cases_match_reference_build(gpu, ref, size, masked, fma):
+def test_small_cases_match_reference_build(gpu, ref, size, masked):
     w, h = size
     i0, i1, mask, tv, cv = random_case(w, h, seed=w * 7 + h)
     p = params(n_levels=2, n_warp=2, n_iter=7)
     s = run_gpu(i0, i1, mask, tv, cv, p, masked)
-    r = ref.run_ref(i0, i1, mask, tv, cv, p, masked, fma=fma)
-    for name, got, want in (("u", s.copy1DDisparityToHost(), r.copy1DDisparityToHost()),
-                            ("warpUV", s.copyDisparityToHost(), r.copyDisparityToHost())):
-        st = diff_stats(got, want)
-        assert st["max"] <= TOL_MAX, (name, st)
+    r = ref.run_ref(i0, i1, mask, tv, cv, p, masked, fma=False)
+    _exact(s.copy1DDisparityToHost(), r.copy1DDisparityToHost(), "u")
+    _exact(s.copyDisparityToHost(), r.copyDisparityToHost(), "warpUV")
+    for name, comps in (("u_", 1), ("a", 1), ("b", 1), ("c", 1), ("Iu", 1), ("Iz", 1), ("i1warp", 1),
+                        ("tv2", 2), ("p", 2), ("q", 4)):
+        _exact(s.debug_buffer(name, comps), r.plane(name, comps), name)
     r.close()
+    # the shipped build (multiply-add contraction on) differs from it by float32 rounding only
+    rs = ref.run_ref(i0, i1, mask, tv, cv, p, masked, fma=True)
+    assert diff_stats(s.copy1DDisparityToHost(), rs.copy1DDisparityToHost())["max"] <= TOL_MAX
+    rs.close()
 
 
 @pytest.mark.parametrize("masked", [True, False], ids=["masked", "plain"])
 @pytest.mark.parametrize("wh", [(424, 400), (848, 800)])
 def test_benchmark_sizes_match_reference_build(gpu, ref, wh, masked):
     """The synthetic fisheye workloads at 424x400 and 848x800 with the benchmark's solver
-    settings (4 / 5 levels x 3 warps x 50 iterations): max |du| over every pixel."""
+    settings (4 / 5 levels x 3 warps x 50 iterations), every pixel."""
     from vfs_b200 import synth
     w, h = wh
     pair = synth.make_pair(w, h, seed=1000 + w)
     sp = synth.SOLVER_PARAMS
     p = params(beta=sp["beta"], gamma=sp["gamma"], n_levels=synth.n_levels_for(w), n_warp=sp["nWarpIters"],
                n_iter=sp["nSolverIters"], limit_range=synth.LIMIT_RANGE)
-    u = run_gpu(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, masked).copy1DDisparityToHost()
-    r = ref.run_ref(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, masked, fma=False)
-    st = diff_stats(u, r.copy1DDisparityToHost())
-    r.close()
-    assert st["max"] <= TOL_MAX, st
+    s = run_gpu(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, masked)
+    u = s.copy1DDisparityToHost()
+    rn = ref.run_ref(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, masked, fma=False)
+    un = rn.copy1DDisparityToHost()
+    _exact(u, un, "u")
+    _exact(s.copyDisparityToHost(), rn.copyDisparityToHost(), "warpUV")
+    rn.close()
+    rs = ref.run_ref(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, masked, fma=True)
+    us = rs.copy1DDisparityToHost()
+    rs.close()
+    # distance to the shipped build == the reference's own build-to-build spread
+    assert diff_stats(u, us)["max"] <= diff_stats(un, us)["max"]
 
 
 def test_wang_config_matches_reference_build(gpu, ref):
-    """The reference's own Wang fixture and parameters (test_vfs/main.cpp:270-281)."""
+    """The reference's own Wang fixture and parameters (test_vfs/main.cpp:270-281).  Its mask
+    reaches the image border at the coarsest level, where the reference's masked kernels read
+    before their buffers' start (zeros in this build, as in vfs_b200)."""
     d = np.load(os.path.join(os.path.dirname(__file__), "golden", "wang_half", "wang_half.npz"))
     p = params(beta=9.0, gamma=0.85, n_levels=5, n_warp=20, n_iter=10, limit_range=0.1)
     mask = d["mask_u8"].astype(np.float32) / 255.0
     u = run_gpu(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True).copy1DDisparityToHost()
     r = ref.run_ref(d["i0"], d["i1"], mask, d["tv"], d["cv"], p, True, fma=False)
-    st = diff_stats(u, r.copy1DDisparityToHost())
+    _exact(u, r.copy1DDisparityToHost(), "u")
     r.close()
-    assert st["max"] <= TOL_MAX, st
 
 
 def test_state_across_frames_matches_reference_build(gpu, ref):
@@ -89,9 +107,8 @@ def test_state_across_frames_matches_reference_build(gpu, ref):
     p = params(n_levels=2, n_warp=2, n_iter=4)
     s = run_gpu(i0, i1, mask, tv, cv, p, True, frames=3)
     r = ref.run_ref(i0, i1, mask, tv, cv, p, True, frames=3, fma=False)
-    st = diff_stats(s.copy1DDisparityToHost(), r.copy1DDisparityToHost())
+    _exact(s.copy1DDisparityToHost(), r.copy1DDisparityToHost(), "u")
     r.close()
-    assert st["max"] <= TOL_MAX, st
 
 
 def test_output_copies_match_reference_build(gpu, ref):
@@ -102,21 +119,29 @@ def test_output_copies_match_reference_build(gpu, ref):
     s = run_gpu(i0, i1, mask, tv, cv, p, True)
     r = ref.run_ref(i0, i1, mask, tv, cv, p, True, fma=False)
     flow = s.copyDisparityToHost()
-    assert diff_stats(flow, r.copyDisparityToHost())["max"] <= TOL_MAX
-    assert diff_stats(s.copyWarpedImageToHost(), r.copyWarpedImageToHost())["max"] <= 1e-5
+    _exact(flow, r.copyDisparityToHost(), "warpUV")
+    _exact(s.copyWarpedImageToHost(), r.copyWarpedImageToHost(), "warped image")
     # The output kernels are compared on identical input: the reference instance is given the
     # drop-in path's flow before its FlowToHSV and ConvertKB run.
     r.set_plane("warpUV", flow)
     for scale in (1.0, 4.0, 20.0):
-        st = diff_stats(s.copyDisparityVisToHost(scale), r.copyDisparityVisToHost(scale))
-        assert st["max"] <= 1e-6, (scale, st)
+        vs, vr = s.copyDisparityVisToHost(scale), r.copyDisparityVisToHost(scale)
+        # flowToHsv.cu:14-21 indexes its 55-entry colour tables with k0, k1 in 1..55: index 55
+        # (flow angles in the last 1/54 of the wheel) reads past the tables, which is undefined;
+        # vfs_b200 takes the last entry there.  Everywhere else the colours must be identical.
+        du = flow[..., 0].astype(np.float64) / scale
+        dv = flow[..., 1].astype(np.float64) / scale
+        fk = (np.arctan2(-dv, -du) / 3.14159 + 1) / 2 * 54 + 1
+        defined = fk < 54.0 - 1e-4
+        assert defined.mean() > 0.5
+        _exact(vs[defined], vr[defined], f"colour map, flow scale {scale}")
     kb = (45.0, 45.0, 48.0, 32.0, 0.3, -0.1, 0.05, -0.01, 0.064, 0.0, 0.0)
     d_s, X_s = s.copyStereoToHost(*kb)
     d_r, X_r = r.copyStereoToHost(*kb)
     fin = np.isfinite(d_r)
-    assert np.array_equal(fin, np.isfinite(d_s))
-    rel = np.abs(d_s - d_r)[fin] / np.maximum(np.abs(d_r[fin]), 1e-6)
-    assert rel.max() < 1e-5, rel.max()
+    assert np.array_equal(fin, np.isfinite(d_s)) and fin.any()
+    _exact(d_s[fin], d_r[fin], "depth")
+    _exact(X_s[fin], X_r[fin], "X")
     r.close()
 
 
@@ -133,9 +158,8 @@ def test_image_overloads_match_reference_build(gpu, ref, kind):
     p = params(n_levels=2, n_warp=2, n_iter=5)
     s = run_gpu(a, b, mask, tv, cv, p, True)
     r = ref.run_ref(a, b, mask, tv, cv, p, True, fma=False)
-    st = diff_stats(s.copy1DDisparityToHost(), r.copy1DDisparityToHost())
+    _exact(s.copy1DDisparityToHost(), r.copy1DDisparityToHost(), "u")
     r.close()
-    assert st["max"] <= TOL_MAX, st
 
 
 @pytest.mark.parametrize("masked", [True, False], ids=["masked", "plain"])
