@@ -15,6 +15,9 @@ pytestmark = pytest.mark.gpu
 OUT = (("u", 1), ("u_", 1), ("warpUV", 2), ("i1warp", 1), ("Iu", 1), ("Iz", 1), ("Tp", 2), ("a", 1))
 
 
+# the iteration-kernel variants that exist (3-5, 10-11 and 16-17 were removed)
+VARIANTS = (0, 1, 2, 6, 7, 8, 9, 12, 13, 14, 15)
+
 def make(i0, i1, mask, tv, cv, p, fused, half=False, graph=True):
     from vfs_b200.stereotgv import StereoTgv
     s = StereoTgv()
@@ -146,10 +149,8 @@ def test_batch_solve_host_matches_device_path(gpu, one_launch):
 @pytest.mark.parametrize("masked", [True, False])
 def test_every_iteration_variant_bit_identical(gpu, masked):
     """All variants of the fused iteration kernel (shared-memory tiles of 4 / 8 / 16 rows,
-    row-streaming strips of 8 / 16 / 32 rows, 3 to 9 iterations per launch on tiles held in
-    shared memory, two pixels per thread on 62-column tiles, the whole level in the shared
-    memory of a 16- or 8-CTA cluster with two or one cluster barriers per iteration) give the
-    drop-in path's bits
+    3 to 9 iterations per launch on tiles held in shared memory, the whole level in the shared
+    memory of a 16- or 8-CTA cluster) give the drop-in path's bits
     with float storage and one another's bits with half storage, on sizes that cut tiles
     unevenly.  11 iterations per warp leave a remainder after the multi-iteration launches
     of every K (3, 5, 7, 9).  The 64 x 48 case has no row padding at
@@ -164,7 +165,7 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
         solve_frames(ref, i0, i1, masked, 2)
         want = {n: ref.debug_buffer(n, c) for n, c in (("u", 1), ("u_", 1), ("warpUV", 2), ("Tp", 2))}
         half_ref = None
-        for variant in range(18):
+        for variant in VARIANTS:
             s = make(i0, i1, mask, tv, cv, p, fused=True)
             s.set_iteration_variant(variant)
             solve_frames(s, i0, i1, masked, 2)
@@ -177,10 +178,10 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
             if half_ref is None:
                 half_ref = u
             assert np.array_equal(u, half_ref), (w, h, variant, "half")
-    # batched one-launch form with a forced streaming variant
+    # batched one-launch form with a forced 16-row variant
     b = StereoBatch(half_storage=False)
     b.set_mode(True)
-    b.set_iteration_variant(4)
+    b.set_iteration_variant(2)
     members, singles, data = [], [], []
     for k, (w, h, L) in enumerate(cases):
         i0, i1, mask, tv, cv = random_case(w, h, seed=600 + k)
@@ -202,8 +203,7 @@ def test_every_iteration_variant_bit_identical(gpu, masked):
 @pytest.mark.parametrize("masked", [True, False])
 @pytest.mark.parametrize("n_iter", [10, 67])
 def test_cluster_resident_iteration_counts(gpu, masked, n_iter):
-    """The cluster-resident variants (14 / 16: 16 CTAs, 15 / 17: 8 CTAs; two / one cluster
-    barriers per iteration) with an even number of
+    """The cluster-resident variants (14: 16 CTAs, 15: 8 CTAs) with an even number of
     iterations per warp (the results stay in the launch's input buffers) and with more
     iterations than one launch takes (64 + 3), over two frames and with CUDA graphs: the
     drop-in path's bits with float storage, variant 1's bits with half storage.  Heights of
@@ -218,7 +218,7 @@ def test_cluster_resident_iteration_counts(gpu, masked, n_iter):
         href.set_iteration_variant(1)
         solve_frames(href, i0, i1, masked, 2)
         hu = href.copy1DDisparityToHost()
-        for variant in (14, 15, 16, 17):
+        for variant in (14, 15):
             s = make(i0, i1, mask, tv, cv, p, fused=True)
             s.set_iteration_variant(variant)
             solve_frames(s, i0, i1, masked, 2)
@@ -252,7 +252,7 @@ def test_launch_overlap_does_not_change_results(gpu):
 def test_per_level_variants_and_tuned_choice_reported(gpu):
     """A per-level variant list (here one-iteration at full resolution, nine and seven
     iterations per launch below) gives the drop-in path's bits, and the handle reports what
-    it ran; the tuner never picks a row-streaming variant."""
+    it ran; the tuner picks only variants that exist."""
     i0, i1, mask, tv, cv = random_case(120, 90, seed=808)
     p = params(n_levels=3, n_warp=2, n_iter=11)
     ref = make(i0, i1, mask, tv, cv, p, fused=False)
@@ -266,7 +266,18 @@ def test_per_level_variants_and_tuned_choice_reported(gpu):
     t = make(i0, i1, mask, tv, cv, p, fused=True)
     solve_frames(t, i0, i1, True, 1)  # autotuned
     v = t.iteration_variants()
-    assert len(v) == 3 and all(0 <= x < 18 and not 3 <= x <= 5 for x in v)
+    assert len(v) == 3 and all(x in VARIANTS for x in v)
+
+
+def test_retired_variants_are_rejected(gpu):
+    """Numbers of the removed forms (3-5, 10-11, 16-17) and out-of-range numbers are refused."""
+    from vfs_b200.stereotgv import VfsError
+    i0, i1, mask, tv, cv = random_case(64, 48, seed=9)
+    s = make(i0, i1, mask, tv, cv, params(n_levels=1, n_warp=1, n_iter=1), fused=True)
+    for v in (3, 4, 5, 10, 11, 16, 17, 18, -2):
+        with pytest.raises(VfsError):
+            s.set_iteration_variant(v)
+    s.set_iteration_variant(-1)  # back to the tuner
 
 
 @pytest.mark.parametrize("fine,stagger,prio", [(1, 0, 0), (2, 0, 2), (2, 1, 1), (3, 1, 0)])

@@ -287,9 +287,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
           std::vector<float> best_ms(kIterVariants, 1e30f);
           for (int pass = 0; pass < 2; pass++)
           for (int v = 0; v < kIterVariants; v++) {
-            // the row-streaming forms are slower everywhere on B200 (one warp walks its strip
-            // serially); they stay available as forced variants
-            if (v >= kIterFirstRowsVariant && v < kIterFirstTBVariant) continue;
+            if (!iter_variant_valid(v)) continue;
             const int kv = tb_iterations(v);
             if (kv > 1 && (!tb_here || kv > P0.nSolverIters)) continue;
             if (iter_variant_single_pair(v) && na != 1) continue;

@@ -367,7 +367,7 @@ int vfs_set_autotune(vfs_stereo* s, int on) {
 
 int vfs_set_iteration_variant(vfs_stereo* s, int variant) {
   return guarded(s, [&] {
-    if (variant < -1 || variant >= vfs::kIterVariants) throw vfs::ArgError{"iteration variant out of range"};
+    if (variant != -1 && !vfs::iter_variant_valid(variant)) throw vfs::ArgError{"iteration variant out of range or retired"};
     s->impl.engine.forced_variant = variant;
   });
 }
@@ -377,7 +377,7 @@ std::vector<int> checked_levels(const int* variants, int n) {
   if (n < 0 || n > 32 || (n > 0 && !variants)) throw vfs::ArgError{"invalid per-level variant list"};
   std::vector<int> v(variants, variants + n);
   for (int x : v)
-    if (x < 0 || x >= vfs::kIterVariants) throw vfs::ArgError{"iteration variant out of range"};
+    if (!vfs::iter_variant_valid(x)) throw vfs::ArgError{"iteration variant out of range or retired"};
   return v;
 }
 }  // namespace
@@ -400,7 +400,7 @@ int vfs_get_iteration_variants(vfs_stereo* s, int* variants, int max_levels, int
 
 int vfs_batch_set_iteration_variant(vfs_batch* b, int variant) {
   return guarded(b, [&] {
-    if (variant < -1 || variant >= vfs::kIterVariants) throw vfs::ArgError{"iteration variant out of range"};
+    if (variant != -1 && !vfs::iter_variant_valid(variant)) throw vfs::ArgError{"iteration variant out of range or retired"};
     b->engine.forced_variant = variant;
   });
 }

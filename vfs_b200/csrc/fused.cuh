@@ -120,9 +120,6 @@ struct IterArgs {
 // variant selects the tile height (kIterVariantRows[variant] rows of 31 pixels).
 void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
                             int variant);
-// the row-streaming form with `rows` (8, 16 or 32) output rows per warp
-void launch_fused_iteration_rows(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
-                                 int rows);
 
 // ---- K consecutive primal-dual iterations of one pair in one launch (kernels_tb.cu) ----
 constexpr int kIterTBMax = 9;
@@ -159,11 +156,7 @@ void launch_fused_iteration_cluster(const IterCLArgs& A, bool masked, bool half_
 // Fraction of the GPU's resident-block capacity that one launch of a variant for one pair of
 // w x h pixels occupies (1 when it fills or exceeds a wave); the tuner's cost model.
 double iteration_gpu_share(int variant, bool masked, bool half, int w, int h);
-double rows_gpu_share(int variant, bool masked, bool half, int w, int h);
 double tb_gpu_share(int variant, bool masked, bool half, int w, int h);
-double x2_gpu_share(int variant, bool masked, bool half, int w, int h);
-void launch_fused_iteration_x2(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
-                               int variant);
 void launch_fused_iteration_tb(const IterTBArgs& A, bool masked, bool half_storage, cudaStream_t st, int variant);
 
 // ---- per-warp prologue: zero p, q, v-bar; resample tv at x + warpUV; warp I1 ----
@@ -268,34 +261,32 @@ void launch_edge_codes(const float* mask, uint8_t* code, int w, int h, int s, cu
 inline int tiles_x_of(int w) { return (w + kFTW - 1) / kFTW; }
 inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFTH); }
 // the iteration kernel's tiles: 31 x kIterTH pixels (a 32 x (kIterTH + 1) block with halo)
-// Tile-height variants of the iteration kernel (chosen per level by the autotuner in
-// FusedEngine): rows per tile and the minimum resident blocks per SM its launch bounds
-// ask for (which caps registers at 32 or 40 per thread).
-// Variants 0-2: k_fused_iter (32 x (rows + 1) blocks, shared-memory west / north exchange);
-// variants 3-5: k_fused_iter_rows (one warp walks down a 31-column strip of `rows` rows,
-// neighbours by shuffle and registers; kernels_rows.cu).  All give identical results.
-// variants 6-9: k_fused_iter_tb, several iterations per launch with the tile's region in
+// Variants of the iteration kernel (chosen per level by the autotuner in FusedEngine): rows
+// per tile and the minimum resident blocks per SM its launch bounds ask for (which caps
+// registers at 32 or 40 per thread).  All give identical results.
+// Variants 0-2: k_fused_iter (32 x (rows + 1) blocks, shared-memory west / north exchange).
+// Variants 6-9: k_fused_iter_tb, several iterations per launch with the tile's region in
 // shared memory (kernels_tb.cu), one pair per launch only: 3 iterations on 64 x 24 tiles,
 // 5 on 32 x 24, and with one region pixel per thread 3 on 23 x 23 and 5 on 17 x 17 tiles.
-// variants 10-11: k_fused_iter_x2, two horizontally adjacent pixels per thread on 62 x 8 /
-// 62 x 4 tiles (kernels_x2.cu); one pair per launch only.
-// variants 12-13: k_fused_iter_tb with one region pixel per thread, 7 iterations on 11 x 11
+// Variants 12-13: k_fused_iter_tb with one region pixel per thread, 7 iterations on 11 x 11
 // tiles and 9 on 5 x 5 tiles (for the smallest levels, where the GPU is mostly idle).
-// variants 14-15: k_fused_iter_cluster, the whole level in the shared memory of a cluster of
+// Variants 14-15: k_fused_iter_cluster, the whole level in the shared memory of a cluster of
 // 16 / 8 CTAs, all iterations of a warp (up to kCLMaxIters) per launch, two cluster
-// barriers per iteration; variants 16-17: k_fused_iter_cluster1, the same with one cluster
-// barrier per iteration.  Levels that do not fit use the default variant.
+// barriers per iteration.  Levels that do not fit use the default variant.
+// Numbers 3-5, 10-11 and 16-17 belonged to forms that never won on B200 (a warp streaming a
+// row strip, two pixels per thread, one cluster barrier per iteration) and were removed;
+// they are rejected, and the remaining numbers keep their meaning.
 constexpr int kIterVariants = 18;
-constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 8, 16, 32, 24, 24, 23, 17, 8, 4, 11, 5, 0, 0, 0, 0};
-constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 3, 6, 0, 0, 0, 0, 0, 0};
-constexpr int kIterFirstRowsVariant = 3;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 0, 0, 0, 24, 24, 23, 17, 0, 0, 11, 5, 0, 0, 0, 0};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
 constexpr int kIterFirstTBVariant = 6;
-constexpr int kIterFirstX2Variant = 10;
+inline bool iter_variant_retired(int v) { return (v >= 3 && v <= 5) || v == 10 || v == 11 || v == 16 || v == 17; }
+inline bool iter_variant_valid(int v) { return v >= 0 && v < kIterVariants && !iter_variant_retired(v); }
 // variants whose launch carries one pair only (others fall back to the default there)
 inline bool iter_variant_single_pair(int v) { return v >= kIterFirstTBVariant; }
 constexpr int kIterFirstDeepTBVariant = 12;
 constexpr int kIterFirstClusterVariant = 14;
-inline bool iter_variant_cluster(int v) { return v >= kIterFirstClusterVariant && v < kIterVariants; }
+inline bool iter_variant_cluster(int v) { return v == kIterFirstClusterVariant || v == kIterFirstClusterVariant + 1; }
 constexpr int kIterDefaultVariant = 1;
 inline int iter_tiles_x_of(int w) { return (w + 30) / 31; }
 inline int iter_tiles_of(int w, int h, int rows) { return iter_tiles_x_of(w) * ((h + rows - 1) / rows); }

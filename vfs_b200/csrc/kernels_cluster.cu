@@ -32,10 +32,6 @@
 // When the level has no row padding (stride == width), column -1 of a row is the previous
 // row's last pixel, which changes every iteration; the caller then uses this kernel only if
 // no pixel of column 0 is on (StereoTgvImpl::tb_ok), as for the temporally blocked form.
-//
-// k_fused_iter_cluster1 below is the same solve with one cluster barrier per iteration
-// (variants 16-17).  On B200 it measured slower than the two-barrier form, and it is kept
-// as a forced variant.
 #include "common.cuh"
 #include "fused.cuh"
 #include "region_step.cuh"
@@ -55,27 +51,21 @@ constexpr int kCLMaxPixelsPerThread = 3;
 
 struct CLGeometry {
   int rows = 0;         // image rows per CTA
-  int rx = 0, ry = 0;   // region columns (w + 2) and rows (rows + 2; rows + 3 for the one-barrier form)
+  int rx = 0, ry = 0;   // region columns (w + 2) and rows (rows + 2)
   int n = 0;            // elements per array (a multiple of 4)
   size_t bytes = 0;     // dynamic shared memory per CTA
   int ppt = 0;          // owned pixels per thread (1 .. kCLMaxPixelsPerThread)
   int threads = 0;      // threads per CTA
 };
 
-// one: the one-barrier form (two north halo rows, and the incoming rows after the region)
 template <class ST>
-CLGeometry cl_geometry(int ctas, int w, int h, bool one) {
+CLGeometry cl_geometry(int ctas, int w, int h) {
   CLGeometry g;
   g.rows = (h + ctas - 1) / ctas;
   g.rx = w + 2;
-  g.ry = g.rows + (one ? 3 : 2);
+  g.ry = g.rows + 2;
   g.n = ((g.rx * g.ry + 3) / 4) * 4;
   g.bytes = (size_t)g.n * RegionState<ST>::kBytesPerPixel;
-  if (one) {
-    g.bytes = (g.bytes + 15) / 16 * 16 + (size_t)6 * g.rx * (sizeof(float) + sizeof(typename Store2<ST>::T2));
-    // a CTA with a CTA south of it sends its last two rows
-    if (g.rows < 2 && h > g.rows) return CLGeometry{};
-  }
   const int px = g.rows * w;
   for (int k = 1; k <= kCLMaxPixelsPerThread; k++) {
     const int t = ((px + k - 1) / k + 31) / 32 * 32;
@@ -264,179 +254,29 @@ __global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster(const _
   }
 }
 
-// One cluster barrier per iteration (variants 16-17).  The region keeps two halo rows north
-// (rows r0 - 2 and r0 - 1) and one south.  Each CTA also runs the dual step on row r0 - 1,
-// from the same inputs as the CTA that owns it, so the threshold and primal steps of row r0
-// find T p and q of their north neighbours locally: within an iteration only a CTA barrier
-// separates the dual step from the primal step.  After the primal step the edge rows' u-bar
-// and v-bar go to the neighbours' incoming rows (the owner's last two rows south, its first
-// row north), one set per iteration parity; the next iteration copies them into the halo
-// rows after the cluster barrier.  A neighbour's stores of iteration j + 1 therefore never
-// meet the copy of iteration j's rows, and the stores of iteration j + 2 wait for the
-// barrier that ends iteration j + 1.  Every CTA that has a CTA south of it owns at least two
-// rows (the host checks it).
-template <bool MASKED, class ST, int PPT>
-__global__ void __launch_bounds__(kCLMaxThreads, 1) k_fused_iter_cluster1(const __grid_constant__ IterCLArgs A) {
-  typedef Store2<ST> S;
-  typedef typename S::T2 T2;
-  typedef typename S::T4 T4;
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int rank = (int)cluster_rank();
-  if ((int)cluster_size() != A.ctas || (int)(gridDim.x * gridDim.y * gridDim.z) != A.ctas) return;
-
-  const IterPair& P = A.P;
-  const int w = P.w, h = P.h, s = P.s;
-  const int rows = A.rows, RX = w + 2, RY = rows + 3, N = ((RX * RY + 3) / 4) * 4;
-  const int r0 = rank * rows;                  // first owned row; region row ry is image row r0 - 2 + ry
-  const int nown = max(0, min(rows, h - r0));  // owned rows (0 for trailing CTAs)
-  __shared__ int s_geo[4];  // north rank or -1, south rank or -1, first owned row, last owned row
-  if (threadIdx.x == 0) {
-    s_geo[0] = (rank > 0 && nown > 0) ? rank - 1 : -1;
-    s_geo[1] = (rank + 1 < A.ctas && (rank + 1) * rows < h) ? rank + 1 : -1;
-    s_geo[2] = nown > 0 ? r0 : -1;
-    s_geo[3] = nown > 0 ? r0 + nown - 1 : -1;
-  }
-  const volatile int* geo = s_geo;
-  RegionState<ST> R;
-  R.carve(smem, N);
-  // incoming halo rows [parity][slot][RX]: slots 0, 1 = rows r0 - 2, r0 - 1; slot 2 = row r0 + nown
-  float* in_ub = reinterpret_cast<float*>(smem + ((size_t)N * RegionState<ST>::kBytesPerPixel + 15) / 16 * 16);
-  T2* in_v = reinterpret_cast<T2*>(in_ub + 6 * RX);
-  auto to = [](const void* local, int rank_to) { return cluster_addr(local, (unsigned)rank_to); };
-
-  const int plane = s * h;
-  const T2* pin = (const T2*)P.p + (A.parity ? plane : 0);
-  const T4* qin = (const T4*)P.q + (A.parity ? plane : 0);
-  const int tid = (int)threadIdx.x, nthr = (int)blockDim.x;
-  griddep_wait();
-
-  if (nown > 0)
-    for (int l = tid; l < RX * (nown + 3); l += nthr) {
-      const int ry = l / RX, rx = l - ry * RX;
-      R.template load<MASKED>(P, pin, qin, ry * RX + rx, rx - 1, r0 - 2 + ry);
-    }
-  int pi[PPT], pxy[PPT];
-#pragma unroll
-  for (int k = 0; k < PPT; k++) {
-    const int l = tid + k * nthr;
-    const int ry = l / max(w, 1), rx = l - ry * w;
-    const bool own = l < nown * w;
-    pi[k] = own ? (ry + 2) * RX + rx + 1 : -1;
-    pxy[k] = own ? rx | ((r0 + ry) << 16) : 0;
-  }
-  cluster_barrier();  // every CTA has started and loaded its halo rows
-
-#pragma unroll 1
-  for (int j = 0; j < A.n; j++) {
-    // ---- the neighbours' edge rows of the last iteration into the halo rows -------------
-    if (j > 0) {
-      const int par = (j - 1) & 1, north = geo[0], south = geo[1];
-      for (int x = tid; x < w; x += nthr) {
-        if (north >= 0) {
-          R.ub[x + 1] = in_ub[(par * 3 + 0) * RX + x + 1];
-          R.v[x + 1] = in_v[(par * 3 + 0) * RX + x + 1];
-          R.ub[RX + x + 1] = in_ub[(par * 3 + 1) * RX + x + 1];
-          R.v[RX + x + 1] = in_v[(par * 3 + 1) * RX + x + 1];
-        }
-        if (south >= 0) {
-          R.ub[(nown + 2) * RX + x + 1] = in_ub[(par * 3 + 2) * RX + x + 1];
-          R.v[(nown + 2) * RX + x + 1] = in_v[(par * 3 + 2) * RX + x + 1];
-        }
-      }
-      __syncthreads();
-    }
-    // ---- dual step on row r0 - 1 (a copy of the north CTA's) and on the owned rows -------
-    if (geo[0] >= 0)
-      for (int x = tid; x < w; x += nthr) R.template dual<MASKED>(RX + x + 1, RX, x, r0 - 1, w, h, A.sp[j], A.sq[j]);
-#pragma unroll 1
-    for (int k = 0; k < PPT; k++) {
-      const int i = pi[k];
-      if (i < 0) continue;
-      R.template dual<MASKED>(i, RX, pxy[k] & 0xffff, pxy[k] >> 16, w, h, A.sp[j], A.sq[j]);
-    }
-    __syncthreads();
-    // ---- threshold and primal steps; the edge rows' u-bar and v-bar to the neighbours ------
-    const int par = j & 1;
-#pragma unroll 1
-    for (int k = 0; k < PPT; k++) {
-      const int i = pi[k];
-      if (i < 0) continue;
-      const int gx = pxy[k] & 0xffff, gy = pxy[k] >> 16;
-      if (MASKED && !(R.code[i] & kOn)) R.keep(i);
-      else R.template primal<MASKED>(P, i, RX, gx, gy, A.tau[j], A.mu[j]);
-      const int north = geo[0], south = geo[1], first = geo[2], last = geo[3];
-      int slot = -1, to_rank = -1;
-      if (north >= 0 && gy == first) {
-        slot = 2;
-        to_rank = north;
-      }
-      if (slot >= 0) {
-        st_cluster(to(in_ub + (par * 3 + slot) * RX + gx + 1, to_rank), R.ub[i]);
-        st_cluster(to(in_v + (par * 3 + slot) * RX + gx + 1, to_rank), R.v[i]);
-      }
-      slot = -1;
-      if (south >= 0 && gy == last - 1) slot = 0;
-      if (south >= 0 && gy == last) slot = 1;
-      if (slot >= 0) {
-        st_cluster(to(in_ub + (par * 3 + slot) * RX + gx + 1, south), R.ub[i]);
-        st_cluster(to(in_v + (par * 3 + slot) * RX + gx + 1, south), R.v[i]);
-      }
-    }
-    // column -1 of the owned rows and of row r0 - 1 is never written: it alternates
-    if (MASKED) {
-      for (int r = tid; r < nown; r += nthr) R.keep((r + 2) * RX);
-      if (tid == 0 && geo[0] >= 0) R.keep(RX);
-    }
-    cluster_barrier();
-  }
-
-  const bool odd = A.n & 1;
-  float* uo = odd ? P.us : const_cast<float*>(P.u);
-  float* ubo = odd ? P.u_s : const_cast<float*>(P.u_);
-  T2* vo = (T2*)(odd ? P.v_s : const_cast<void*>(P.v_));
-  const int pl = (A.parity + A.n) & 1;
-  T2* po = (T2*)P.p + (pl ? plane : 0);
-  T4* qo = (T4*)P.q + (pl ? plane : 0);
-#pragma unroll
-  for (int k = 0; k < PPT; k++) {
-    const int i = pi[k];
-    if (i < 0) continue;
-    if (MASKED && !(R.code[i] & kOn)) continue;
-    const int pos = (pxy[k] & 0xffff) + (pxy[k] >> 16) * s;
-    uo[pos] = R.u[i];
-    ubo[pos] = R.ub[i];
-    vo[pos] = R.v[i];
-    po[pos] = R.p[i];
-    qo[pos] = S::rnd4(R.q[i]);
-    if (A.write_tp) P.Tp[pos] = R.tp[i];
-  }
-}
-
 namespace {
 
 typedef void (*CLKernel)(IterCLArgs);
 
-template <bool ONE, bool MASKED, class ST, int PPT>
+template <bool MASKED, class ST, int PPT>
 CLKernel cl_kernel() {
-  if constexpr (ONE) return k_fused_iter_cluster1<MASKED, ST, PPT>;
-  else return k_fused_iter_cluster<MASKED, ST, PPT>;
+  return k_fused_iter_cluster<MASKED, ST, PPT>;
 }
 
-// Dynamic shared memory a CTA of the kernels may use: the device's opt-in maximum less the
-// larger static shared memory of the two forms.
+// Dynamic shared memory a CTA of the kernel may use: the device's opt-in maximum less the
+// kernel's static shared memory.
 int max_dynamic_smem() {
   int dev = 0, optin = 0;
   VFS_CUDA(cudaGetDevice(&dev));
   VFS_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-  cudaFuncAttributes f0{}, f1{};
+  cudaFuncAttributes f0{};
   VFS_CUDA(cudaFuncGetAttributes(&f0, k_fused_iter_cluster<true, float, 1>));
-  VFS_CUDA(cudaFuncGetAttributes(&f1, k_fused_iter_cluster1<true, float, 1>));
-  return optin - (int)std::max(f0.sharedSizeBytes, f1.sharedSizeBytes);
+  return optin - (int)f0.sharedSizeBytes;
 }
 
-template <bool ONE, bool MASKED, class ST, int PPT>
+template <bool MASKED, class ST, int PPT>
 void set_cl_attributes() {
-  const CLKernel k = cl_kernel<ONE, MASKED, ST, PPT>();
+  const CLKernel k = cl_kernel<MASKED, ST, PPT>();
   static std::atomic<bool> configured[kMaxDevices];
   int dev = 0;
   VFS_CUDA(cudaGetDevice(&dev));
@@ -464,23 +304,23 @@ cudaLaunchConfig_t cl_config(const CLGeometry& g, int ctas, cudaStream_t st, cud
 }
 
 // can a cluster of this shape be resident on the device (0 or the number of such clusters)
-template <bool ONE, bool MASKED, class ST, int PPT>
+template <bool MASKED, class ST, int PPT>
 int cl_max_clusters(const CLGeometry& g, int ctas) {
-  set_cl_attributes<ONE, MASKED, ST, PPT>();
+  set_cl_attributes<MASKED, ST, PPT>();
   cudaLaunchAttribute at[2];
   unsigned nat = 0;
   cudaLaunchConfig_t cfg = cl_config(g, ctas, 0, at, nat);
   int n = 0;
-  if (cudaOccupancyMaxActiveClusters(&n, cl_kernel<ONE, MASKED, ST, PPT>(), &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&n, cl_kernel<MASKED, ST, PPT>(), &cfg) != cudaSuccess) {
     (void)cudaGetLastError();
     return 0;
   }
   return n;
 }
 
-template <bool ONE, bool MASKED, class ST, int PPT>
+template <bool MASKED, class ST, int PPT>
 void launch_cl(const IterCLArgs& A, const CLGeometry& g, int ctas, cudaStream_t st) {
-  set_cl_attributes<ONE, MASKED, ST, PPT>();
+  set_cl_attributes<MASKED, ST, PPT>();
   cudaLaunchAttribute at[2];
   unsigned nat = 0;
   cudaLaunchConfig_t cfg = cl_config(g, ctas, st, at, nat);
@@ -491,47 +331,41 @@ void launch_cl(const IterCLArgs& A, const CLGeometry& g, int ctas, cudaStream_t 
     nat++;
     cfg.numAttrs = nat;
   }
-  VFS_CUDA(cudaLaunchKernelEx(&cfg, cl_kernel<ONE, MASKED, ST, PPT>(), A));
+  VFS_CUDA(cudaLaunchKernelEx(&cfg, cl_kernel<MASKED, ST, PPT>(), A));
 }
 
-// run F<ONE, MASKED, ST, PPT> for the runtime form, storage and pixels per thread
-template <template <bool, bool, class, int> class F, typename... Args>
-auto cl_dispatch(bool one, bool masked, bool half, int ppt, Args&&... args) {
-#define VFS_CL_PPT(O, M, T)                                   \
+// run F<MASKED, ST, PPT> for the runtime form, storage and pixels per thread
+template <template <bool, class, int> class F, typename... Args>
+auto cl_dispatch(bool masked, bool half, int ppt, Args&&... args) {
+#define VFS_CL_PPT(M, T)                                      \
   switch (ppt) {                                              \
-    case 1: return F<O, M, T, 1>::run(args...);               \
-    case 2: return F<O, M, T, 2>::run(args...);               \
-    case 3: return F<O, M, T, 3>::run(args...);               \
+    case 1: return F<M, T, 1>::run(args...);                  \
+    case 2: return F<M, T, 2>::run(args...);                  \
+    case 3: return F<M, T, 3>::run(args...);                  \
     default: throw ArgError{"cluster-resident iteration: level too large"}; \
   }
-#define VFS_CL_ST(O, M) \
-  if (half) { VFS_CL_PPT(O, M, __half) } else { VFS_CL_PPT(O, M, float) }
-#define VFS_CL_M(O) \
-  if (masked) { VFS_CL_ST(O, true) } else { VFS_CL_ST(O, false) }
-  if (one) { VFS_CL_M(true) } else { VFS_CL_M(false) }
-#undef VFS_CL_M
+#define VFS_CL_ST(M) \
+  if (half) { VFS_CL_PPT(M, __half) } else { VFS_CL_PPT(M, float) }
+  if (masked) { VFS_CL_ST(true) } else { VFS_CL_ST(false) }
 #undef VFS_CL_ST
 #undef VFS_CL_PPT
 }
 
-template <bool ONE, bool MASKED, class ST, int PPT>
+template <bool MASKED, class ST, int PPT>
 struct MaxClusters {
-  static int run(const CLGeometry& g, int ctas) { return cl_max_clusters<ONE, MASKED, ST, PPT>(g, ctas); }
+  static int run(const CLGeometry& g, int ctas) { return cl_max_clusters<MASKED, ST, PPT>(g, ctas); }
 };
-template <bool ONE, bool MASKED, class ST, int PPT>
+template <bool MASKED, class ST, int PPT>
 struct Launch {
   static int run(const IterCLArgs& A, const CLGeometry& g, int ctas, cudaStream_t st) {
-    launch_cl<ONE, MASKED, ST, PPT>(A, g, ctas, st);
+    launch_cl<MASKED, ST, PPT>(A, g, ctas, st);
     return 0;
   }
 };
 
-bool one_barrier(int variant) { return variant >= kIterFirstClusterVariant + 2; }
-
 CLGeometry geometry_of(int variant, bool half, int w, int h) {
   const int ctas = cluster_ctas(variant);
-  const bool one = one_barrier(variant);
-  return half ? cl_geometry<__half>(ctas, w, h, one) : cl_geometry<float>(ctas, w, h, one);
+  return half ? cl_geometry<__half>(ctas, w, h) : cl_geometry<float>(ctas, w, h);
 }
 
 }  // namespace
@@ -540,8 +374,6 @@ int cluster_ctas(int variant) {
   switch (variant) {
     case kIterFirstClusterVariant: return 16;
     case kIterFirstClusterVariant + 1: return 8;
-    case kIterFirstClusterVariant + 2: return 16;
-    case kIterFirstClusterVariant + 3: return 8;
     default: return 0;
   }
 }
@@ -563,7 +395,7 @@ bool cluster_fits(int variant, bool masked, bool half, int w, int h) {
   const CLGeometry g = geometry_of(variant, half, w, h);
   // (a thread packs a pixel's column and row into one int: 16 bits each)
   bool ok = g.ppt > 0 && g.bytes <= (size_t)max_dynamic_smem() && w + 2 <= 4096 && h < 32768;
-  if (ok) ok = cl_dispatch<MaxClusters>(one_barrier(variant), masked, half, g.ppt, g, ctas) >= 1;
+  if (ok) ok = cl_dispatch<MaxClusters>(masked, half, g.ppt, g, ctas) >= 1;
   std::lock_guard<std::mutex> lk(mu);
   known[key] = ok;
   return ok;
@@ -592,7 +424,7 @@ void launch_fused_iteration_cluster(const IterCLArgs& A, bool masked, bool half_
   if (A.P.w <= 0 || A.P.h <= 0) return;
   const CLGeometry g = geometry_of(variant, half_storage, A.P.w, A.P.h);
   if (A.rows != g.rows || A.ctas != ctas || g.ppt == 0) throw ArgError{"cluster-resident iteration: bad geometry"};
-  cl_dispatch<Launch>(one_barrier(variant), masked, half_storage, g.ppt, A, g, ctas, st);
+  cl_dispatch<Launch>(masked, half_storage, g.ppt, A, g, ctas, st);
   VFS_LAUNCH_CHECK();
 }
 

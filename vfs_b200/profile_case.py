@@ -8,13 +8,13 @@ unless --autotune 1, so the launch sequence is fixed).
 
 Launch order per frame: pyramid, then per level (coarse to fine) the level kernels and per
 warp the prologue, the fused iterations and the epilogue.  With the default iteration
-variant (or --variant 0..5) each warp has 50 one-iteration launches: in the concurrent mode
+variant (or --variant 0..2) each warp has 50 one-iteration launches: in the concurrent mode
 each pair's solve is enqueued in turn (pair 0 first), so k_fused_iter launches 600..749 are
 pair 0's full-resolution iterations (one pair per launch); in the one-launch mode every
 launch carries all pairs, and launches 600..749 are the full-resolution iterations of the
 batch.  With --variant 6..9 or 12..13 (K iterations per launch) each warp has 50 / K launches
-of k_fused_iter_tb, coarsest level first; with --variant 14..17 each warp of a level that fits
-a cluster's shared memory has one launch of k_fused_iter_cluster (k_fused_iter_cluster1 for 16..17).
+of k_fused_iter_tb, coarsest level first; with --variant 14..15 each warp of a level that fits
+a cluster's shared memory has one launch of k_fused_iter_cluster.
 """
 from __future__ import annotations
 
