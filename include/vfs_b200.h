@@ -247,6 +247,11 @@ int vfs_equalize_hist_u8_noalloc(const uint8_t* d_src, uint8_t* d_dst, size_t n,
  * vfs_profile_read() sums the records of a group kind (0 = drop-in inner iteration,
  * 1 = fused inner launch, 2 = fused per-warp prologue, 3 = fused epilogue). */
 long long vfs_launch_count(void);
+
+/* Device-side status of the current device (no counterpart in the reference): *status = 1 if
+ * a kernel of the TMA-staged iteration variant gave up a bounded wait for its copies since the
+ * last call (its block then wrote nothing), else 0; the flag is cleared.  Synchronous. */
+int vfs_device_status(int* status);
 /* Process-wide: launch the fused iteration kernels with programmatic dependent launch
  * (on = 1, the default), so that each launch is scheduled while the previous one drains;
  * every such kernel waits for its predecessor's results before reading memory, so the

@@ -16,7 +16,7 @@ OUT = (("u", 1), ("u_", 1), ("warpUV", 2), ("i1warp", 1), ("Iu", 1), ("Iz", 1), 
 
 
 # the iteration-kernel variants that exist (3-5, 10-11 and 16-17 were removed)
-VARIANTS = (0, 1, 2, 6, 7, 8, 9, 12, 13, 14, 15)
+VARIANTS = (0, 1, 2, 6, 7, 8, 9, 12, 13, 14, 15, 18)
 
 def make(i0, i1, mask, tv, cv, p, fused, half=False, graph=True):
     from vfs_b200.stereotgv import StereoTgv
@@ -150,7 +150,7 @@ def test_batch_solve_host_matches_device_path(gpu, one_launch):
 def test_every_iteration_variant_bit_identical(gpu, masked):
     """All variants of the fused iteration kernel (shared-memory tiles of 4 / 8 / 16 rows,
     3 to 9 iterations per launch on tiles held in shared memory, the whole level in the shared
-    memory of a 16- or 8-CTA cluster) give the drop-in path's bits
+    memory of a 16- or 8-CTA cluster, 8-row tiles staged by TMA) give the drop-in path's bits
     with float storage and one another's bits with half storage, on sizes that cut tiles
     unevenly.  11 iterations per warp leave a remainder after the multi-iteration launches
     of every K (3, 5, 7, 9).  The 64 x 48 case has no row padding at
@@ -379,3 +379,27 @@ def test_batch_solve_device_matches_host_buffers(gpu):
         torch.cuda.synchronize()
         for k, (g, w_) in enumerate(zip(d_out, want)):
             assert np.array_equal(g.cpu().numpy(), w_), (frame, k)
+
+
+@pytest.mark.parametrize("half", [False, True], ids=["fp32", "fp16"])
+def test_tma_iteration_matches_default_at_full_size(gpu, half):
+    """The TMA-staged iteration kernel (variant 18) on a synthetic 848 x 800 fisheye pair, every
+    level: the bits of the default variant (and, with float storage, of the drop-in path); the
+    kernel's bounded copy waits never ran out."""
+    import ctypes
+    from vfs_b200 import synth
+    from vfs_b200._native import lib
+    pair = synth.make_pair(848, 800, seed=4242)
+    sp = synth.SOLVER_PARAMS
+    p = params(beta=sp["beta"], gamma=sp["gamma"], n_levels=synth.n_levels_for(848), n_warp=sp["nWarpIters"],
+               n_iter=sp["nSolverIters"], limit_range=synth.LIMIT_RANGE)
+    out = {}
+    for v in (1, 18):
+        s = make(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, fused=True, half=half)
+        s.set_iteration_variant(v)
+        solve_frames(s, pair.i0, pair.i1, True, 2)
+        out[v] = (s.copy1DDisparityToHost(), s.debug_buffer("warpUV", 2))
+        assert s.iteration_variants() == [v] * synth.n_levels_for(848)
+    assert np.array_equal(out[1][0], out[18][0]) and np.array_equal(out[1][1], out[18][1])
+    st = ctypes.c_int(-1)
+    assert lib().vfs_device_status(ctypes.byref(st)) == 0 and st.value == 0

@@ -90,6 +90,7 @@ SIGNATURES = {
     "vfs_equalize_hist_u8_noalloc": [_vp, _vp, _sz, _i, _vp],
     "vfs_estimate_device_bytes": [_i, _i, _i, _f, _i, _i],
     "vfs_launch_count": [],
+    "vfs_device_status": [_vp],
     "vfs_set_launch_overlap": [_i],
     "vfs_profile_enable": [_vp, _i],
     "vfs_profile_reset": [_vp],

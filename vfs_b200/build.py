@@ -21,7 +21,7 @@ LIB = os.path.join(OUT_DIR, "libvfs_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
                      "-Xcompiler", "-Wall", "--expt-relaxed-constexpr"]
-SOURCES = ["kernels_plain.cu", "kernels_hist.cu", "kernels_fused.cu", "kernels_tb.cu", "kernels_cluster.cu", "stereo_tgv.cu", "batch.cu",
+SOURCES = ["kernels_plain.cu", "kernels_hist.cu", "kernels_fused.cu", "kernels_tb.cu", "kernels_cluster.cu", "kernels_tma.cu", "stereo_tgv.cu", "batch.cu",
            "capi.cu", "io.cpp"]
 
 

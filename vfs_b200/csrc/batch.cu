@@ -208,11 +208,13 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         }
         A.npairs = na;
         A.span_rows = 0;
-        if (na == 1 && masked && variant >= 0 && variant < 3) {
+        // the TMA variant has the 8-row tiles of variant 1, and its tile spans
+        const int sv = variant == kIterTmaVariant ? 1 : variant;
+        if (na == 1 && masked && sv >= 0 && sv < 3) {
           const StereoTgvImpl* s = act[0];
-          if (level < (int)s->span_lo[variant].size()) {
-            const std::vector<uint16_t>& lo = s->span_lo[variant][level];
-            const std::vector<uint16_t>& hi = s->span_hi[variant][level];
+          if (level < (int)s->span_lo[sv].size()) {
+            const std::vector<uint16_t>& lo = s->span_lo[sv][level];
+            const std::vector<uint16_t>& hi = s->span_hi[sv][level];
             if (!lo.empty() && (int)lo.size() <= kMaxSpanRows) {
               A.span_rows = (int)lo.size();
               A.span_max = 0;
@@ -228,6 +230,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
       };
       // the K-iterations-per-launch kernel: one pair per launch, and exact at this level
       const bool tb_here = na == 1 && (!masked || (level < (int)act[0]->tb_ok.size() && act[0]->tb_ok[level]));
+      const bool tma_here = na == 1 && (!masked || (level < (int)act[0]->tma_ok.size() && act[0]->tma_ok[level]));
       auto tb_args = [&](float sigma_, float tau_, int iter0, int k) {
         IterTBArgs T{};
         T.P = iter_args(kIterDefaultVariant, sigma_, tau_, 1.0f, 0).pr[0];
@@ -291,6 +294,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             const int kv = tb_iterations(v);
             if (kv > 1 && (!tb_here || kv > P0.nSolverIters)) continue;
             if (iter_variant_single_pair(v) && na != 1) continue;
+            if (v == kIterTmaVariant && !tma_here) continue;
             const bool clv = iter_variant_cluster(v);
             if (clv && (!tb_here || !cluster_fits(v, masked, half, lw, lh))) continue;
             // the cluster-resident kernel is timed over an odd number of iterations, so that it
@@ -303,6 +307,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             auto once = [&] {
               if (clv) launch_fused_iteration_cluster(CL, masked, half, st, v);
               else if (kv > 1) launch_fused_iteration_tb(TB, masked, half, st, v);
+              else if (v == kIterTmaVariant) launch_fused_iteration_tma(T, masked, half, st, 0);
               else launch_fused_iteration(T, masked, half, st, 0, v);
             };
             once();  // warm the caches / the instruction path
@@ -340,7 +345,8 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
       const bool cl_here = tb_here && iter_variant_cluster(variant) && cluster_fits(variant, masked, half, lw, lh);
       const int K = cl_here ? kCLMaxIters : tb_here ? tb_iterations(variant) : 1;
       const int v1 = (tb_iterations(variant) > 1 || iter_variant_cluster(variant) ||
-                      (iter_variant_single_pair(variant) && na != 1))
+                      (iter_variant_single_pair(variant) && na != 1) ||
+                      (variant == kIterTmaVariant && !tma_here))
                          ? kIterDefaultVariant
                          : variant;
       float tau = 1.0f;
@@ -371,7 +377,8 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
           if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P0.timestep_lambda);
           else mu = 1;
           IterArgs A = iter_args(v1, sigma, tau, mu, iter == n_it - 1);
-          launch_fused_iteration(A, masked, half, st, iter & 1, v1);
+          if (v1 == kIterTmaVariant) launch_fused_iteration_tma(A, masked, half, st, iter & 1);
+          else launch_fused_iteration(A, masked, half, st, iter & 1, v1);
           sigma = sigma / mu;
           tau = tau * mu;
         }
@@ -508,6 +515,7 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
       // the multi-iteration kernel cannot follow that pixel, so it is used there only when
       // no pixel of column 0 is on
       s->tb_ok.assign(s->levels(), 1);
+      s->tma_ok.assign(s->levels(), 1);
       for (int v = 0; v < 3; v++) {
         s->span_lo[v].assign(s->levels(), {});
         s->span_hi[v].assign(s->levels(), {});
@@ -518,9 +526,11 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
         VFS_CUDA(cudaMemcpy2DAsync(code.data(), w, s->code_masked[l], s->pS[l], w, h, cudaMemcpyDeviceToHost,
                                    s->stream()));
         VFS_CUDA(cudaStreamSynchronize(s->stream()));
-        if (w == s->pS[l])
-          for (int y = 0; y < h; y++)
-            if (code[(size_t)y * w] & kOn) s->tb_ok[l] = 0;
+        for (int y = 0; y < h; y++)
+          if (code[(size_t)y * w] & kOn) {
+            s->tma_ok[l] = 0;
+            if (w == s->pS[l]) s->tb_ok[l] = 0;
+          }
         // first and last on column of every image row
         std::vector<int> xmin(h, w), xmax(h, -1);
         for (int y = 0; y < h; y++)

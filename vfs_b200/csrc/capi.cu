@@ -634,6 +634,18 @@ int vfs_equalize_hist_u8(const uint8_t* d_src, uint8_t* d_dst, size_t n, void* c
 
 long long vfs_launch_count(void) { return vfs::launch_counter().load(); }
 
+int vfs_device_status(int* status) {
+  try {
+    int v = vfs::tma_status_take();
+    if (status) *status = v;
+    return VFS_OK;
+  } catch (const vfs::CudaError& e) {
+    (void)cudaGetLastError();
+    vfs::set_global_error(cudaGetErrorString(e.err));
+    return VFS_ERR_CUDA;
+  }
+}
+
 int vfs_set_launch_overlap(int on) {
   vfs::pdl_enabled().store(on != 0);
   return VFS_OK;

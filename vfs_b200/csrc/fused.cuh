@@ -158,6 +158,12 @@ void launch_fused_iteration_cluster(const IterCLArgs& A, bool masked, bool half_
 double iteration_gpu_share(int variant, bool masked, bool half, int w, int h);
 double tb_gpu_share(int variant, bool masked, bool half, int w, int h);
 void launch_fused_iteration_tb(const IterTBArgs& A, bool masked, bool half_storage, cudaStream_t st, int variant);
+// one iteration of one pair with its region staged by TMA (variant 18, kernels_tma.cu); A is
+// laid out as for variant 1 (8-row tiles, tile spans)
+void launch_fused_iteration_tma(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity);
+double tma_gpu_share(bool masked, bool half, int w, int h);
+// reads and clears the device status of the TMA iteration kernel (1: a bounded wait ran out)
+int tma_status_take();
 
 // ---- per-warp prologue: zero p, q, v-bar; resample tv at x + warpUV; warp I1 ----
 struct WarpStartPair {
@@ -273,12 +279,16 @@ inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFT
 // Variants 14-15: k_fused_iter_cluster, the whole level in the shared memory of a cluster of
 // 16 / 8 CTAs, all iterations of a warp (up to kCLMaxIters) per launch, two cluster
 // barriers per iteration.  Levels that do not fit use the default variant.
+// Variant 18: k_fused_iter_tma (kernels_tma.cu), the 8-row tiles of variant 1 with every input
+// plane of the block's region brought into shared memory by bulk tensor copies (TMA); one pair
+// per launch, on levels where no pixel of column 0 is on (masked form).
 // Numbers 3-5, 10-11 and 16-17 belonged to forms that never won on B200 (a warp streaming a
 // row strip, two pixels per thread, one cluster barrier per iteration) and were removed;
 // they are rejected, and the remaining numbers keep their meaning.
-constexpr int kIterVariants = 18;
-constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 0, 0, 0, 24, 24, 23, 17, 0, 0, 11, 5, 0, 0, 0, 0};
-constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+constexpr int kIterVariants = 19;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 0, 0, 0, 24, 24, 23, 17, 0, 0, 11, 5, 0, 0, 0, 0, 8};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+constexpr int kIterTmaVariant = 18;
 constexpr int kIterFirstTBVariant = 6;
 inline bool iter_variant_retired(int v) { return (v >= 3 && v <= 5) || v == 10 || v == 11 || v == 16 || v == 17; }
 inline bool iter_variant_valid(int v) { return v >= 0 && v < kIterVariants && !iter_variant_retired(v); }

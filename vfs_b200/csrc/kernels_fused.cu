@@ -287,6 +287,8 @@ double iteration_gpu_share(int variant, bool masked, bool half, int w, int h) {
   int per_sm = 0;
   if (iter_variant_cluster(variant)) {
     return cluster_gpu_share(variant, w, h);
+  } else if (variant == kIterTmaVariant) {
+    return tma_gpu_share(masked, half, w, h);
   } else if (variant >= kIterFirstTBVariant) {
     return tb_gpu_share(variant, masked, half, w, h);
   } else {
@@ -309,7 +311,7 @@ void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, c
                             int variant) {
   if (A.ntiles <= 0) return;
   static_assert(kIterVariantRows[0] == 4 && kIterVariantRows[1] == 8 && kIterVariantRows[2] == 16, "variants");
-  if (iter_variant_retired(variant)) throw ArgError{"retired iteration variant"};
+  if (iter_variant_retired(variant) || variant == kIterTmaVariant) throw ArgError{"not a k_fused_iter variant"};
   switch (variant) {
     case 0: launch_iter_th<4, kIterVariantMinBlocks[0]>(A, masked, half_storage, st, parity); break;
     case 2: launch_iter_th<16, kIterVariantMinBlocks[2]>(A, masked, half_storage, st, parity); break;

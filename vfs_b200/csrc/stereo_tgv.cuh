@@ -132,6 +132,10 @@ class StereoTgvImpl {
   // per level: the K-iterations-per-launch kernel reproduces the masked form exactly (false
   // only when the row has no padding and a pixel of column 0 is on; kernels_tb.cu)
   std::vector<uint8_t> tb_ok;
+  // per level (masked form): no pixel of column 0 is on, so no pixel reads west of the image
+  // (where the reference reads the previous row's last element); the TMA iteration kernel,
+  // whose copies are two-dimensional, is used only there
+  std::vector<uint8_t> tma_ok;
   // per one-iteration tile variant (0-2) and level: for each tile row, the first and last
   // tile column whose region (tile + west / north halo) holds a pixel that is on (masked
   // form; first > last for a row without any)
