@@ -274,7 +274,7 @@ def test_retired_variants_are_rejected(gpu):
     from vfs_b200.stereotgv import VfsError
     i0, i1, mask, tv, cv = random_case(64, 48, seed=9)
     s = make(i0, i1, mask, tv, cv, params(n_levels=1, n_warp=1, n_iter=1), fused=True)
-    for v in (3, 4, 5, 10, 11, 16, 17, 18, -2):
+    for v in (3, 4, 5, 10, 11, 16, 17, 19, -2):
         with pytest.raises(VfsError):
             s.set_iteration_variant(v)
     s.set_iteration_variant(-1)  # back to the tuner
