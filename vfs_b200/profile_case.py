@@ -4,7 +4,7 @@ unless --autotune 1, so the launch sequence is fixed).
 
     python -m vfs_b200.profile_case --batch 4 --half 1 [--frames 1] [--path fused|plain]
                                     [--mode concurrent|one_launch] [--autotune 0|1]
-                                    [--variant -1..17] [--variants 1,1,8,9,9]
+                                    [--variant -1..18] [--variants 1,1,8,9,9]
 
 Launch order per frame: pyramid, then per level (coarse to fine) the level kernels and per
 warp the prologue, the fused iterations and the epilogue.  With the default iteration
