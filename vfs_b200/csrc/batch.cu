@@ -230,11 +230,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
       };
       // the K-iterations-per-launch kernel: one pair per launch, and exact at this level
       const bool tb_here = na == 1 && (!masked || (level < (int)act[0]->tb_ok.size() && act[0]->tb_ok[level]));
-      const int mk = masked ? 1 : 0;
-      const bool tma_here = na == 1 && (!masked || (level < (int)act[0]->tma_ok.size() && act[0]->tma_ok[level])) &&
-                            level < (int)act[0]->tma_seg_n[mk].size();
-      const uint32_t* tma_seg = tma_here ? act[0]->d_tma_seg + act[0]->tma_seg_off[mk][level] : nullptr;
-      const int tma_nseg = tma_here ? act[0]->tma_seg_n[mk][level] : 0;
+      const bool tma_here = na == 1 && (!masked || (level < (int)act[0]->tma_ok.size() && act[0]->tma_ok[level]));
       auto tb_args = [&](float sigma_, float tau_, int iter0, int k) {
         IterTBArgs T{};
         T.P = iter_args(kIterDefaultVariant, sigma_, tau_, 1.0f, 0).pr[0];
@@ -311,7 +307,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             auto once = [&] {
               if (clv) launch_fused_iteration_cluster(CL, masked, half, st, v);
               else if (kv > 1) launch_fused_iteration_tb(TB, masked, half, st, v);
-              else if (v == kIterTmaVariant) launch_fused_iteration_tma(T, tma_seg, tma_nseg, masked, half, st, 0);
+              else if (v == kIterTmaVariant) launch_fused_iteration_tma(T, masked, half, st, 0);
               else launch_fused_iteration(T, masked, half, st, 0, v);
             };
             once();  // warm the caches / the instruction path
@@ -326,9 +322,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             if (pass == 0) continue;
             ms = best_ms[v];
             double share = 1.0;
-            if (na == 1)
-              share = v == kIterTmaVariant ? tma_gpu_share(masked, half, tma_nseg)
-                                           : iteration_gpu_share(v, masked, half, lw, lh);
+            if (na == 1) share = iteration_gpu_share(v, masked, half, lw, lh);
             double cost = (double)ms * std::max(share, floor_share);
             // the default keeps its place unless another variant is clearly (5 %) cheaper
             if (v == kIterDefaultVariant) cost *= 0.95;
@@ -383,7 +377,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
           if (sigma < 1000.0f) mu = 1.0f / std::sqrt(1 + 0.7f * tau * P0.timestep_lambda);
           else mu = 1;
           IterArgs A = iter_args(v1, sigma, tau, mu, iter == n_it - 1);
-          if (v1 == kIterTmaVariant) launch_fused_iteration_tma(A, tma_seg, tma_nseg, masked, half, st, iter & 1);
+          if (v1 == kIterTmaVariant) launch_fused_iteration_tma(A, masked, half, st, iter & 1);
           else launch_fused_iteration(A, masked, half, st, iter & 1, v1);
           sigma = sigma / mu;
           tau = tau * mu;
@@ -570,7 +564,6 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
           s->span_hi[v][l] = hi;
         }
       }
-      s->buildTmaSegments(true);
       s->codes_valid = true;
       s->generation = next_generation();  // graphs captured under the old mask are not reused
     }

@@ -16,8 +16,6 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <vector>
-
 namespace vfs {
 
 constexpr int kMaxPairs = 24;
@@ -160,17 +158,10 @@ void launch_fused_iteration_cluster(const IterCLArgs& A, bool masked, bool half_
 double iteration_gpu_share(int variant, bool masked, bool half, int w, int h);
 double tb_gpu_share(int variant, bool masked, bool half, int w, int h);
 void launch_fused_iteration_tb(const IterTBArgs& A, bool masked, bool half_storage, cudaStream_t st, int variant);
-// one iteration of one pair, persistent blocks over the segments of 8-row tiles seg[0 .. nseg)
-// (device memory, built by tma_segments), each tile's region staged by TMA (variant 18,
-// kernels_tma.cu); A is laid out as for variant 1
-void launch_fused_iteration_tma(const IterArgs& A, const uint32_t* seg, int nseg, bool masked, bool half_storage,
-                                cudaStream_t st, int parity);
-double tma_gpu_share(bool masked, bool half, int nseg);
-// segments (column, first row, rows) of a w x h level's active 8-row tiles; lo / hi: first and
-// last active tile column of every tile row (nullptr: every tile is active)
-std::vector<uint32_t> tma_segments(int w, int h, const uint16_t* lo, const uint16_t* hi);
-// most segments a level with row pitch s and height h can have
-size_t tma_segment_capacity(int s, int h);
+// one iteration of one pair with its region staged by TMA (variant 18, kernels_tma.cu); A is
+// laid out as for variant 1 (8-row tiles, tile spans)
+void launch_fused_iteration_tma(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity);
+double tma_gpu_share(bool masked, bool half, int w, int h);
 // reads and clears the device status of the TMA iteration kernel (1: a bounded wait ran out)
 int tma_status_take();
 

@@ -287,7 +287,8 @@ double iteration_gpu_share(int variant, bool masked, bool half, int w, int h) {
   int per_sm = 0;
   if (iter_variant_cluster(variant)) {
     return cluster_gpu_share(variant, w, h);
-
+  } else if (variant == kIterTmaVariant) {
+    return tma_gpu_share(masked, half, w, h);
   } else if (variant >= kIterFirstTBVariant) {
     return tb_gpu_share(variant, masked, half, w, h);
   } else {

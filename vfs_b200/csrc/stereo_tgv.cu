@@ -106,11 +106,6 @@ void StereoTgvImpl::release() {
   pool_ = nullptr;
   if (fpool_) cudaFree(fpool_);
   fpool_ = nullptr;
-  d_tma_seg = nullptr;
-  for (int m = 0; m < 2; m++) {
-    tma_seg_off[m].clear();
-    tma_seg_n[m].clear();
-  }
   f_p = f_q = f_vh = f_vhs = nullptr;
   code_masked.clear();
   code_plain.clear();
@@ -146,10 +141,7 @@ static size_t pool_bytes_for(const std::vector<int>& pS, const std::vector<int>&
 static size_t fused_bytes_for(const std::vector<int>& pS, const std::vector<int>& pH, size_t full) {
   size_t bytes = full * 2 * 8 + full * 2 * 16 + full * 4 * 2 + 8 * 512;
   for (size_t l = 0; l < pS.size(); l++) bytes += 2 * ((size_t)pS[l] * pH[l] + 512);
-  // segment lists of the TMA iteration kernel, both forms
-  size_t segs = 0;
-  for (size_t l = 0; l < pS.size(); l++) segs += 2 * tma_segment_capacity(pS[l], pH[l]);
-  return bytes + segs * sizeof(uint32_t) + 512;
+  return bytes;
 }
 
 size_t estimate_device_bytes(int width, int height, int nLevels, float fScale, int sa, bool fused) {
@@ -374,41 +366,9 @@ void StereoTgvImpl::ensureFused() {
     code_masked[l] = (uint8_t*)take((size_t)pS[l] * pH[l]);
     code_plain[l] = (uint8_t*)take((size_t)pS[l] * pH[l]);
   }
-  size_t segs = 0;
-  for (int l = 0; l < levels(); l++) segs += 2 * tma_segment_capacity(pS[l], pH[l]);
-  d_tma_seg = (uint32_t*)take(segs * sizeof(uint32_t));
-  int seg_off = 0;
-  for (int m = 0; m < 2; m++) {
-    tma_seg_off[m].assign(levels(), 0);
-    tma_seg_n[m].assign(levels(), 0);
-    for (int l = 0; l < levels(); l++) {
-      tma_seg_off[m][l] = seg_off;
-      seg_off += (int)tma_segment_capacity(pS[l], pH[l]);
-    }
-  }
   VFS_CUDA(cudaMemsetAsync(fpool_, 0, bytes, stream_));
   for (int l = 0; l < levels(); l++) launch_edge_codes(nullptr, code_plain[l], pW[l], pH[l], pS[l], stream_);
   codes_valid = false;
-  buildTmaSegments(false);
-}
-
-void StereoTgvImpl::buildTmaSegments(bool masked) {
-  const int m = masked ? 1 : 0;
-  std::vector<std::vector<uint32_t>> lists(levels());
-  for (int l = 0; l < levels(); l++) {
-    if (masked) {
-      if (l >= (int)span_lo[1].size() || span_lo[1][l].empty()) continue;
-      lists[l] = tma_segments(pW[l], pH[l], span_lo[1][l].data(), span_hi[1][l].data());
-    } else {
-      lists[l] = tma_segments(pW[l], pH[l], nullptr, nullptr);
-    }
-    if (lists[l].size() > tma_segment_capacity(pS[l], pH[l])) throw ArgError{"TMA segment list overflow"};
-    tma_seg_n[m][l] = (int)lists[l].size();
-    if (!lists[l].empty())
-      VFS_CUDA(cudaMemcpyAsync(d_tma_seg + tma_seg_off[m][l], lists[l].data(), lists[l].size() * sizeof(uint32_t),
-                               cudaMemcpyHostToDevice, stream_));
-  }
-  VFS_CUDA(cudaStreamSynchronize(stream_));  // the host lists die here
 }
 
 // stereotgv.cu:389-515 (masked) and 256-387 (plain).  Pointer swaps are the

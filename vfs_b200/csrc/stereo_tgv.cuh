@@ -136,13 +136,6 @@ class StereoTgvImpl {
   // (where the reference reads the previous row's last element); the TMA iteration kernel,
   // whose copies are two-dimensional, is used only there
   std::vector<uint8_t> tma_ok;
-  // segment lists of the TMA iteration kernel (in the fused pool), per form (0 plain, 1
-  // masked) and level: offset in elements and count
-  uint32_t* d_tma_seg = nullptr;
-  std::vector<int> tma_seg_off[2], tma_seg_n[2];
-  // builds form `masked`'s segment lists (spans of the 8-row tiles for the masked form) and
-  // copies them to the device on the handle's stream; blocks until they are there
-  void buildTmaSegments(bool masked);
   // per one-iteration tile variant (0-2) and level: for each tile row, the first and last
   // tile column whose region (tile + west / north halo) holds a pixel that is on (masked
   // form; first > last for a row without any)
