@@ -166,8 +166,9 @@ __global__ void __launch_bounds__(32 * (kTH + 1), 6) k_fused_iter_tma(const __gr
     tma_load_2d(sm.Iu, &A.m_Iu, xs, y0, bar);
     tma_load_2d(sm.Iz, &A.m_Iz, xs, y0, bar);
   }
-  if (!mbar_wait_bounded(bar)) {
-    atomicExch(&g_tma_status, 1);
+  // the block decides together whether the copies landed (a block barrier follows later)
+  if (__syncthreads_or(!mbar_wait_bounded(bar))) {
+    if (tid == 0) atomicExch(&g_tma_status, 1);
     (void)mbar_wait_bounded(bar);  // give copies still in flight a last bounded chance to land
     return;
   }
