@@ -65,6 +65,30 @@ int vfs_set_camera(vfs_stereo* s, float baseline, float focal);
  * reference's CUDA build.  VFS_TENSOR_MATH_PORTABLE uses an exp / log built only from
  * correctly rounded IEEE operations, which a CPU restatement reproduces bit for bit; the two
  * weights agree to 1.5e-6 relative.  Applies to both solve paths from the next solve on. */
+/* Warm start (no counterpart in the reference, which starts every solve from zero:
+ * stereotgv.cu:395-397).  level < 0 (the default): off.  level >= 0: once the handle has solved
+ * a frame, the next solve starts at pyramid level min(level, nLevels - 1), 0 being full
+ * resolution, from the previous frame's disparity (box-downscaled to that level); the levels
+ * above it are not solved.  level = nLevels - 1 keeps every level and only changes the starting
+ * point.  initialize and loadVectorFields forget the previous frame. */
+int vfs_set_warm_start(vfs_stereo* s, int level);
+
+/* Whole-state export / import (no counterpart in the reference): the handle's device state
+ * (image pyramid, mask, fields, every solver buffer with the stale values the reference keeps
+ * between frames, and the warm-start disparity), so that a handle initialised with the same
+ * size, levels and scale continues bit for bit where the exported one stopped; a camera
+ * stream's state can thus leave the GPU while the stream is idle.  Host-side settings (limit
+ * range, camera, solve path, stream) are not part of it.  vfs_state_bytes gives the size (0 before
+ * initialize); both calls synchronise the handle's stream. */
+size_t vfs_state_bytes(const vfs_stereo* s);
+int vfs_export_state(vfs_stereo* s, void* host, size_t bytes);
+int vfs_import_state(vfs_stereo* s, const void* host, size_t bytes);
+
+/* Test hook (no counterpart in the reference): with n > 0 the n-th following device-pool
+ * allocation of any handle fails as if the GPU were out of memory (the call returns
+ * VFS_ERR_NOMEM and leaves nothing allocated); 0 turns it off. */
+int vfs_debug_fail_allocation(int n);
+
 #define VFS_TENSOR_MATH_CUDA 0
 #define VFS_TENSOR_MATH_PORTABLE 1
 int vfs_set_tensor_math(vfs_stereo* s, int mode);

@@ -45,6 +45,11 @@ SIGNATURES = {
     "vfs_set_limit_range": [_vp, _f],
     "vfs_set_camera": [_vp, _f, _f],
     "vfs_set_tensor_math": [_vp, _i],
+    "vfs_set_warm_start": [_vp, _i],
+    "vfs_state_bytes": [_vp],
+    "vfs_export_state": [_vp, _vp, _sz],
+    "vfs_import_state": [_vp, _vp, _sz],
+    "vfs_debug_fail_allocation": [_i],
     "vfs_get_level_size": [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)],
     "vfs_load_vector_fields": [_vp, _vp, _vp],
     "vfs_copy_mask_to_device": [_vp, _vp],
@@ -106,6 +111,7 @@ SIGNATURES = {
 _RESTYPE = {
     "vfs_estimate_device_bytes": ctypes.c_size_t,
     "vfs_launch_count": ctypes.c_longlong,
+    "vfs_state_bytes": ctypes.c_size_t,
     "vfs_status_string": ctypes.c_char_p,
     "vfs_last_error": ctypes.c_char_p,
     "vfs_batch_last_error": ctypes.c_char_p,

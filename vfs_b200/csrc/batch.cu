@@ -58,15 +58,21 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     maxL = std::max(maxL, s->levels());
   }
   StereoTgvImpl* prof = pairs[0];
+  // first level of each pair: its coarsest, or the level a warm start begins at
+  std::vector<int> top(n);
+  for (int k = 0; k < n; k++) top[k] = pairs[k]->topLevel();
+  auto top_of = [&](const StereoTgvImpl* s) {
+    for (int k = 0; k < n; k++)
+      if (pairs[k] == s) return top[k];
+    return s->levels() - 1;
+  };
   // ---- calibration warp, state reset, image pyramid (stereotgv.cu:392-405) ---------
   if (part != 2) {
-  for (auto* s : pairs) {
+  for (int k = 0; k < n; k++) {
+    StereoTgvImpl* s = pairs[k];
     launch_warp_image(s->tex1(s->pI1[0], 0), s->d_cv, s->d_i1calibrated, s->geomAt(0), st);
     std::swap(s->pI1[0], s->d_i1calibrated);
-    size_t f = s->fullElems() * sizeof(float);
-    VFS_CUDA(cudaMemsetAsync(s->d_u, 0, f, st));
-    VFS_CUDA(cudaMemsetAsync(s->d_u_, 0, f, st));
-    VFS_CUDA(cudaMemsetAsync(s->d_warpUV, 0, 2 * f, st));
+    s->startState(top[k], st);
   }
   for (int l = 1; l < maxL; l++) {
     DownArgs D{};
@@ -92,8 +98,9 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   for (int level = maxL - 1; level >= 0; level--) {
     if ((part == 1 && level == 0) || (part == 2 && level > 0)) continue;
     std::vector<StereoTgvImpl*> act;
-    for (auto* s : pairs)
-      if (level < s->levels()) act.push_back(s);
+    for (int k = 0; k < n; k++)
+      if (level <= top[k]) act.push_back(pairs[k]);
+    if (act.empty()) continue;
     const int na = (int)act.size();
     long long px_level = 0;
     for (auto* s : act) px_level += (long long)s->pW[level] * s->pH[level];
@@ -112,7 +119,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         d.warpUV = s->d_warpUV;
         d.u = s->d_u;
         d.tv = s->pTvF[level];
-        d.init_flow = level == s->levels() - 1;
+        d.init_flow = level == top_of(s);
         d.w = s->pW[level];
         d.h = s->pH[level];
         d.s = s->pS[level];
@@ -571,6 +578,13 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
 }
 
 void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st, int part) {
+  solve_parts(pairs, masked, half, st, part);
+  if (part != 1)
+    for (auto* s : pairs) s->have_prev = true;  // the frame's disparity is in d_u (warm starts)
+}
+
+void FusedEngine::solve_parts(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st,
+                              int part) {
   if (pairs.empty()) return;
   prepare(pairs, masked);
   // tile variants per level for this batch composition (tuned on its first solve)
@@ -588,7 +602,10 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   const bool forced = forced_variant >= 0 || !forced_levels.empty();
   if (tit == tuned_.end())
     tit = tuned_.emplace(comp, std::vector<int>(maxL, (autotune && !forced) ? -1 : kIterDefaultVariant)).first;
-  auto in_part = [&](int l) { return !((part == 1 && l == 0) || (part == 2 && l > 0)); };
+  // levels a warm start skips are not run (and not tuned) in this solve
+  int max_top = 0;
+  for (auto* s : pairs) max_top = std::max(max_top, s->topLevel());
+  auto in_part = [&](int l) { return !((part == 1 && l == 0) || (part == 2 && l > 0)) && l <= max_top; };
   bool need_tune = false;
   if (autotune && !forced) {
     // a composition tuned before (by any engine of the process) is reused, so that every
@@ -639,6 +656,7 @@ void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
     const uintptr_t* w = reinterpret_cast<const uintptr_t*>(&p);
     key.push_back((uintptr_t)s);
     key.push_back((uintptr_t)s->generation);
+    key.push_back((uintptr_t)s->topLevel());
     key.insert(key.end(), w, w + sizeof(PairPtrs) / sizeof(uintptr_t));
     uint32_t lr;
     std::memcpy(&lr, &s->P.limitRange, 4);

@@ -170,6 +170,29 @@ int vfs_set_limit_range(vfs_stereo* s, float lr) {
   });
 }
 
+int vfs_set_warm_start(vfs_stereo* s, int level) {
+  return guarded(s, [&] {
+    if (level < -1) throw vfs::ArgError{"vfs_set_warm_start: level must be -1 (off) or >= 0"};
+    s->impl.warm_level = level;
+  });
+}
+
+size_t vfs_state_bytes(const vfs_stereo* s) { return s ? s->impl.stateBytes() : 0; }
+
+int vfs_export_state(vfs_stereo* s, void* host, size_t bytes) {
+  return guarded(s, [&] { s->impl.exportState(host, bytes); });
+}
+
+int vfs_import_state(vfs_stereo* s, const void* host, size_t bytes) {
+  return guarded(s, [&] { s->impl.importState(host, bytes); });
+}
+
+int vfs_debug_fail_allocation(int n) {
+  if (n < 0) return VFS_ERR_ARG;
+  vfs::alloc_failure_countdown().store(n);
+  return VFS_OK;
+}
+
 int vfs_set_tensor_math(vfs_stereo* s, int mode) {
   return guarded(s, [&] {
     if (mode != VFS_TENSOR_MATH_CUDA && mode != VFS_TENSOR_MATH_PORTABLE)

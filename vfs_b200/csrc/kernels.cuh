@@ -21,6 +21,8 @@ void launch_pack_tight(const float* src, float* dst, int comps, Geom g, cudaStre
 // downscale.cu:10-30 (float) / :98-122 (float2): mean of 4 taps at +-1/4 coarse px
 void launch_downscale(cudaTextureObject_t fine, int comps, float* out, Geom coarse, cudaStream_t st);
 // downscale.cu:52-73 point-sampled (mask pyramid)
+// 2 x 2 box to the next coarser level with the values multiplied by `scale` (warm start)
+void launch_downscale_scaled(cudaTextureObject_t fine, float* out, float scale, Geom g, cudaStream_t st);
 void launch_downscale_nearest(cudaTextureObject_t fine, float* out, Geom coarse, cudaStream_t st);
 // warpImage.cu:9-23
 void launch_warp_image(cudaTextureObject_t src, const float2* warpUV, float* out, Geom g, cudaStream_t st);

@@ -60,6 +60,20 @@ __global__ void k_cv8uc3_to_gray(const uchar3* src, float* dst, Geom g) {
   dst[idx] = v / 256.0f;
 }
 
+// Warm start: the previous frame's disparity one level coarser, the same 2 x 2 box as
+// k_downscale1, with the values scaled to the coarser level's pixels (x scale).
+__global__ void k_downscale_scaled(cudaTextureObject_t fine, float* out, float scale, Geom g) {
+  int ix, iy;
+  if (!pixel(ix, iy, g.w, g.h)) return;
+  float dx = 1.0f / (float)g.w, dy = 1.0f / (float)g.h;
+  float x = ((float)ix + 0.5f) * dx, y = ((float)iy + 0.5f) * dy;
+  float t1 = tex2D<float>(fine, x - dx * 0.25f, y);
+  float t2 = tex2D<float>(fine, x + dx * 0.25f, y);
+  float t3 = tex2D<float>(fine, x, y - dy * 0.25f);
+  float t4 = tex2D<float>(fine, x, y + dy * 0.25f);
+  out[ix + iy * g.s] = 0.25f * (t1 + t2 + t3 + t4) * scale;
+}
+
 __global__ void k_downscale1(cudaTextureObject_t fine, float* out, Geom g) {
   int ix, iy;
   if (!pixel(ix, iy, g.w, g.h)) return;
@@ -496,6 +510,10 @@ void launch_cv8uc3_to_gray(const uchar3* src, float* dst, Geom g, cudaStream_t s
 void launch_downscale(cudaTextureObject_t fine, int comps, float* out, Geom g, cudaStream_t st) {
   if (comps == 2) k_downscale2<<<L2D(g)>>>(fine, (float2*)out, g);
   else k_downscale1<<<L2D(g)>>>(fine, out, g);
+  VFS_LAUNCH_CHECK();
+}
+void launch_downscale_scaled(cudaTextureObject_t fine, float* out, float scale, Geom g, cudaStream_t st) {
+  k_downscale_scaled<<<L2D(g)>>>(fine, out, scale, g);
   VFS_LAUNCH_CHECK();
 }
 void launch_downscale_nearest(cudaTextureObject_t fine, float* out, Geom g, cudaStream_t st) {

@@ -5,6 +5,8 @@
 
 #include "stereo_tgv.cuh"
 
+#include <atomic>
+
 namespace vfs {
 
 StereoTgvImpl::StereoTgvImpl(int bw, int bh, int sa) : blockWidth(bw), blockHeight(bh), strideAlignment(sa) {}
@@ -99,6 +101,24 @@ void StereoTgvImpl::profRead(int tag, long long* count, double* total_ms, double
   if (pixel_iters) *pixel_iters = pi;
 }
 
+// Test hook (vfs_debug_fail_allocation): when n > 0, the n-th following device-pool allocation
+// of any handle fails as if the device were out of memory.
+std::atomic<int>& alloc_failure_countdown() {
+  static std::atomic<int> n{0};
+  return n;
+}
+
+static cudaError_t pool_malloc(void** p, size_t bytes) {
+  int n = alloc_failure_countdown().load();
+  while (n > 0 && !alloc_failure_countdown().compare_exchange_weak(n, n - 1)) {
+  }
+  if (n == 1) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
 void StereoTgvImpl::release() {
   engine.clear();
   tex.clear();
@@ -167,6 +187,7 @@ void StereoTgvImpl::initialize(const SolverParams& p) {
     throw ArgError{"initialize: invalid size or iteration count"};
   if (strideAlignment <= 0 || blockWidth <= 0 || blockHeight <= 0)
     throw ArgError{"initialize: invalid block or stride alignment"};
+  have_prev = false;
   release();
   if (!stream_) stream_ = own_stream();
   generation = next_generation();
@@ -198,7 +219,7 @@ void StereoTgvImpl::initialize(const SolverParams& p) {
     throw ArgError{"initialize: image too large (row pitch x height x 8 must stay below 2^31)"};
   size_t f = full_ * sizeof(float);
   pool_bytes_ = pool_bytes_for(pS, pH, full_);
-  cudaError_t e = cudaMalloc(&pool_, pool_bytes_);
+  cudaError_t e = pool_malloc((void**)&pool_, pool_bytes_);
   if (e != cudaSuccess) {
     pool_ = nullptr;
     (void)cudaGetLastError();
@@ -262,6 +283,7 @@ void StereoTgvImpl::initialize(const SolverParams& p) {
 // stereotgv.cu:171-199.  The reference also builds a negated copy of the field
 // (pTvBackward) that the solver never reads; it is not kept here.
 void StereoTgvImpl::loadVectorFields(const float* tv, const float* cvf) {
+  have_prev = false;  // a warm start follows the fields it was solved with
   if (!initialized_) throw ArgError{"loadVectorFields before initialize"};
   if (!tv || !cvf) throw ArgError{"loadVectorFields: null field"};
   size_t row = (size_t)width * sizeof(float2);
@@ -334,7 +356,24 @@ void StereoTgvImpl::solve(bool masked) {
     engine.solve(one, masked, half_storage, stream_);
   } else {
     solveReference(masked);
+    have_prev = true;
   }
+}
+
+void StereoTgvImpl::startState(int top, cudaStream_t st) {
+  const size_t f = full_ * sizeof(float);
+  if (!(warm_level >= 0 && have_prev)) {  // stereotgv.cu:395-397
+    VFS_CUDA(cudaMemsetAsync(d_u, 0, f, st));
+    VFS_CUDA(cudaMemsetAsync(d_u_, 0, f, st));
+    VFS_CUDA(cudaMemsetAsync(d_warpUV, 0, 2 * f, st));
+    return;
+  }
+  for (int l = 1; l <= top; l++) {
+    launch_downscale_scaled(t1(d_u, l - 1), d_us, 1.0f / P.fScale, geom(l), st);
+    std::swap(d_u, d_us);
+  }
+  launch_clone(d_u_, d_u, geom(top), st);
+  VFS_CUDA(cudaMemsetAsync(d_warpUV, 0, 2 * f, st));
 }
 
 // Fused-path buffers: p and q in two planes each (float: 8 + 16 bytes per pixel per
@@ -343,7 +382,7 @@ void StereoTgvImpl::ensureFused() {
   if (fpool_) return;
   size_t n = full_;
   size_t bytes = fused_bytes_for(pS, pH, full_);
-  cudaError_t e = cudaMalloc(&fpool_, bytes);
+  cudaError_t e = pool_malloc((void**)&fpool_, bytes);
   if (e != cudaSuccess) {
     fpool_ = nullptr;
     (void)cudaGetLastError();
@@ -379,19 +418,18 @@ void StereoTgvImpl::solveReference(bool masked) {
   const size_t f = full_ * sizeof(float);
   launch_warp_image(t1(pI1[0], 0), d_cv, d_i1calibrated, geom(0), st);
   std::swap(pI1[0], d_i1calibrated);
-  VFS_CUDA(cudaMemsetAsync(d_u, 0, f, st));
-  VFS_CUDA(cudaMemsetAsync(d_u_, 0, f, st));
-  VFS_CUDA(cudaMemsetAsync(d_warpUV, 0, 2 * f, st));
+  const int top = topLevel();
+  startState(top, st);
   for (int l = 1; l < P.nLevels; l++) {
     launch_downscale(t1(pI0[l - 1], l - 1), 1, pI0[l], geom(l), st);
     launch_downscale(t1(pI1[l - 1], l - 1), 1, pI1[l], geom(l), st);
   }
-  for (int level = P.nLevels - 1; level >= 0; level--) {
+  for (int level = top; level >= 0; level--) {
     Geom g = geom(level);
     const float* mk = masked ? pMask[level] : nullptr;
     for (float* b : {d_a, d_b, d_c, d_etau, d_etav1, d_etav2, d_i0smooth}) VFS_CUDA(cudaMemsetAsync(b, 0, f, st));
     const float eta_p = 3.0f, eta_q = 2.0f;
-    if (level == P.nLevels - 1) launch_optical_flow_vector(d_u, pTvF[level], d_warpUV, g, st);
+    if (level == top) launch_optical_flow_vector(d_u, pTvF[level], d_warpUV, g, st);
     launch_gaussian(t1(pI0[level], level), mk, d_i0smooth, g, st);
     int xcov = ((g.h + blockWidth - 1) / blockWidth) * blockWidth;  // calcTensor.cu:81,227
     launch_calc_tensor(t1(d_i0smooth, level), mk, P.beta, P.gamma, d_a, d_b, d_c, g, std::min(g.w, xcov),
@@ -447,6 +485,105 @@ void StereoTgvImpl::solveReference(bool masked) {
       std::swap(d_warpUV, d_warpUVs);
     }
   }
+}
+
+// ---- state export / import ----------------------------------------------------------
+namespace {
+constexpr uint32_t kStateMagic = 0x53534656u;  // "VFSS"
+constexpr uint32_t kStateVersion = 1;
+constexpr int kStateRoles = 12;
+struct StateHeader {
+  uint32_t magic, version;
+  int32_t width, height, stride, levels, stride_alignment, has_fused;
+  float fScale;
+  int32_t f_parity, have_prev, reserved;
+  uint64_t pool_bytes, fpool_bytes;
+  int64_t role[kStateRoles];  // byte offsets in their pool (the last two: the fused pool); -1 = null
+};
+}  // namespace
+
+size_t StereoTgvImpl::stateBytes() const {
+  if (!initialized_) return 0;
+  return sizeof(StateHeader) + pool_bytes_ + (fpool_ ? fused_bytes_for(pS, pH, full_) : 0);
+}
+
+void StereoTgvImpl::exportState(void* host, size_t bytes) {
+  if (!initialized_) throw ArgError{"export_state before initialize"};
+  if (!host) throw ArgError{"export_state: null buffer"};
+  const size_t need = stateBytes();
+  if (bytes < need) throw ArgError{"export_state: buffer smaller than vfs_state_bytes"};
+  const size_t fbytes = fpool_ ? fused_bytes_for(pS, pH, full_) : 0;
+  StateHeader h{};
+  h.magic = kStateMagic;
+  h.version = kStateVersion;
+  h.width = width;
+  h.height = height;
+  h.stride = stride;
+  h.levels = levels();
+  h.stride_alignment = strideAlignment;
+  h.has_fused = fpool_ ? 1 : 0;
+  h.fScale = P.fScale;
+  h.f_parity = f_parity;
+  h.have_prev = have_prev ? 1 : 0;
+  h.pool_bytes = pool_bytes_;
+  h.fpool_bytes = fbytes;
+  const void* roles[kStateRoles] = {pI1[0], d_i1calibrated, d_u, d_us, d_u_, d_u_s,
+                                    d_v_, d_v_s, d_warpUV, d_warpUVs, f_vh, f_vhs};
+  for (int k = 0; k < kStateRoles; k++) {
+    const char* base = k < 10 ? pool_ : fpool_;
+    h.role[k] = roles[k] ? (int64_t)((const char*)roles[k] - base) : -1;
+  }
+  VFS_CUDA(cudaStreamSynchronize(stream_));
+  char* out = (char*)host;
+  std::memcpy(out, &h, sizeof(h));
+  VFS_CUDA(cudaMemcpy(out + sizeof(h), pool_, pool_bytes_, cudaMemcpyDeviceToHost));
+  if (fbytes) VFS_CUDA(cudaMemcpy(out + sizeof(h) + pool_bytes_, fpool_, fbytes, cudaMemcpyDeviceToHost));
+}
+
+void StereoTgvImpl::importState(const void* host, size_t bytes) {
+  if (!initialized_) throw ArgError{"import_state before initialize"};
+  if (!host || bytes < sizeof(StateHeader)) throw ArgError{"import_state: no state"};
+  StateHeader h;
+  std::memcpy(&h, host, sizeof(h));
+  if (h.magic != kStateMagic || h.version != kStateVersion) throw ArgError{"import_state: not a vfs_b200 state"};
+  if (h.width != width || h.height != height || h.stride != stride || h.levels != levels() ||
+      h.stride_alignment != strideAlignment || h.fScale != P.fScale || h.pool_bytes != pool_bytes_)
+    throw ArgError{"import_state: the handle's geometry differs from the exported one"};
+  const size_t fbytes = fused_bytes_for(pS, pH, full_);
+  if (bytes != sizeof(h) + h.pool_bytes + h.fpool_bytes || (h.has_fused && h.fpool_bytes != fbytes))
+    throw ArgError{"import_state: size mismatch"};
+  for (int k = 0; k < kStateRoles; k++) {
+    const uint64_t lim = k < 10 ? h.pool_bytes : h.fpool_bytes;
+    if (h.role[k] < -1 || (h.role[k] >= 0 && (uint64_t)h.role[k] >= lim))
+      throw ArgError{"import_state: corrupt buffer roles"};
+  }
+  if (h.has_fused) ensureFused();
+  VFS_CUDA(cudaStreamSynchronize(stream_));
+  const char* in = (const char*)host + sizeof(h);
+  VFS_CUDA(cudaMemcpy(pool_, in, pool_bytes_, cudaMemcpyHostToDevice));
+  if (h.has_fused) VFS_CUDA(cudaMemcpy(fpool_, in + pool_bytes_, fbytes, cudaMemcpyHostToDevice));
+  auto at = [&](int k) -> void* {
+    if (h.role[k] < 0) return nullptr;
+    return (k < 10 ? pool_ : fpool_) + h.role[k];
+  };
+  pI1[0] = (float*)at(0);
+  d_i1calibrated = (float*)at(1);
+  d_u = (float*)at(2);
+  d_us = (float*)at(3);
+  d_u_ = (float*)at(4);
+  d_u_s = (float*)at(5);
+  d_v_ = (float2*)at(6);
+  d_v_s = (float2*)at(7);
+  d_warpUV = (float2*)at(8);
+  d_warpUVs = (float2*)at(9);
+  if (h.has_fused) {
+    f_vh = at(10);
+    f_vhs = at(11);
+  }
+  f_parity = h.f_parity;
+  have_prev = h.have_prev != 0;
+  codes_valid = false;  // the masked edge codes and tile spans are derived again from the mask
+  generation = next_generation();
 }
 
 // stereotgv.cu:517-568 outputs: level-0 views of u, warpUV, the warped image.

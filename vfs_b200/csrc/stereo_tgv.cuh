@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -53,6 +54,9 @@ class FusedEngine {
   void clear();
   // part: 0 whole solve; 1 everything before the full-resolution level; 2 that level alone
   void solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st, int part = 0);
+ private:
+  void solve_parts(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st, int part);
+ public:
   // allocate fused buffers and refresh edge codes, each on the pair's own stream
   static void prepare(std::vector<StereoTgvImpl*>& pairs, bool masked);
   size_t graphs() const { return cache_.size(); }
@@ -74,6 +78,8 @@ class FusedEngine {
 
 // process-wide counter of handle states (StereoTgvImpl::generation)
 uint64_t next_generation();
+// allocation-failure injection for tests (vfs_debug_fail_allocation)
+std::atomic<int>& alloc_failure_countdown();
 
 // Device bytes a pair of this geometry allocates: the solver pool, and with `fused`
 // also the fused-path buffers.  Matches StereoTgvImpl::initialize / ensureFused.
@@ -107,6 +113,30 @@ class StereoTgvImpl {
 
   SolverParams P;
   float baseline = 0.0f, focal = 0.0f;
+  // ---- warm start (opt-in; the reference zeroes u, u-bar and warpUV at every solve,
+  // stereotgv.cu:395-397) ---------------------------------------------------------
+  // warm_level < 0: off.  Otherwise, once a frame has been solved, the next solve starts at
+  // pyramid level min(warm_level, levels - 1) from the previous frame's disparity; the levels
+  // above it are skipped.
+  int warm_level = -1;
+  bool have_prev = false;  // d_u holds the disparity of the last solved frame (full resolution)
+  int topLevel() const {
+    return (warm_level >= 0 && have_prev) ? std::min(warm_level, levels() - 1) : levels() - 1;
+  }
+  // State at the start of a solve whose first level is `top`: cold (top = levels - 1 and no
+  // warm start) zeroes u, u-bar and warpUV as the reference does; warm brings the previous
+  // disparity to level `top` (box downscale, values / fScale per level), sets u-bar = u and
+  // zeroes warpUV (the first level derives it from u).
+  void startState(int top, cudaStream_t st);
+
+  // ---- state export / import (no counterpart in the reference) ------------------
+  // The whole device state of the handle (both pools, which physical buffer holds each
+  // ping-pong role, the warm-start flag), so that a handle initialised with the same geometry
+  // continues bit for bit where the exported one stopped.  Host settings (limit range,
+  // camera, solve path, stream) are not part of it.
+  size_t stateBytes() const;
+  void exportState(void* host, size_t bytes);
+  void importState(const void* host, size_t bytes);
   // tensor weight from CUDA's expf / powf as the reference (1, default) or from the portable
   // exp / log of tgv_math.cuh that the CPU oracle restates bit for bit (0)
   int tensor_cuda_math = 1;

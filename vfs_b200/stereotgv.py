@@ -71,6 +71,25 @@ class StereoTgv:
         self._limit_range = float(v)
         check(self._h, self._L.vfs_set_limit_range(self._h, self._limit_range))
 
+    def set_warm_start(self, level: int) -> None:
+        """Start each solve after the first from the previous frame's disparity at pyramid level
+        ``level`` (0 = full resolution; levels above it are skipped); -1 turns it off."""
+        check(self._h, self._L.vfs_set_warm_start(self._h, int(level)))
+
+    def export_state(self) -> np.ndarray:
+        """The handle's whole device state as a byte array (see vfs_export_state)."""
+        n = int(self._L.vfs_state_bytes(self._h))
+        if n == 0:
+            raise VfsError(-3, "export_state before initialize")
+        buf = np.empty(n, np.uint8)
+        check(self._h, self._L.vfs_export_state(self._h, buf.ctypes.data_as(ctypes.c_void_p), n))
+        return buf
+
+    def import_state(self, state: np.ndarray) -> None:
+        """Restore a state exported from a handle of the same size, levels and scale."""
+        buf = np.ascontiguousarray(state, np.uint8)
+        check(self._h, self._L.vfs_import_state(self._h, buf.ctypes.data_as(ctypes.c_void_p), buf.size))
+
     def set_tensor_math(self, portable: bool) -> None:
         """Tensor weight from CUDA's expf / powf as the reference (False, the default) or from
         the portable exp / log that the CPU oracle restates bit for bit (True)."""
