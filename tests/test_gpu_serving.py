@@ -81,3 +81,91 @@ def test_admission_refuses_streams_that_do_not_fit(gpu):
         srv.open_stream(9, 20000, 20000, None, None, None, 8)
     srv.open_stream(0, 96, 80, mask, tv, cv, 2, P)  # admitted once memory is available
     assert 0 in srv.cameras
+
+
+def _alone(sid, w, h, L, frames, mask, tv, cv, half=True):
+    from vfs_b200.serving import StereoServer
+    srv = StereoServer(max_batch=1, lanes=1, half_storage=half, reserve_bytes=0)
+    srv.open_stream(sid, w, h, mask, tv, cv, L, P)
+    reqs = [srv.submit(sid, a, b) for a, b in frames]
+    srv.run_until_idle()
+    return [r.u for r in reqs]
+
+
+def test_parked_stream_continues_bit_for_bit(gpu):
+    """A stream parked to host memory between frames (state exported, device memory freed) and
+    brought back continues exactly where it stopped."""
+    from vfs_b200.serving import StereoServer
+    sid, w, h, L = CAMS[1]
+    fr, mask, tv, cv = _frames(sid, w, h, n=4)
+    want = _alone(sid, w, h, L, fr, mask, tv, cv)
+    srv = StereoServer(max_batch=2, lanes=1, reserve_bytes=0)
+    srv.open_stream(sid, w, h, mask, tv, cv, L, P)
+    got = []
+    for k, (a, b) in enumerate(fr):
+        r = srv.submit(sid, a, b)
+        srv.run_until_idle()
+        got.append(r.u)
+        if k in (1, 2):
+            srv.park_stream(sid)
+            assert srv.cameras[sid].solver is None
+    assert srv.counters["parks"] == 2 and srv.counters["unparks"] == 2
+    for k in range(4):
+        assert np.array_equal(got[k], want[k]), k
+
+
+def test_requests_are_admitted_by_free_memory(gpu):
+    """With room for about one and a half stream states beside the reserve, opening three
+    streams parks the idle ones, and serving their frames parks and brings back states as
+    requests are admitted; every result equals the stream served alone."""
+    import torch
+    from vfs_b200.serving import StereoServer
+    cams = [(10 + k, 256, 200, 3) for k in range(3)]
+    data = {sid: _frames(sid, w, h, n=2) for sid, w, h, _ in cams}
+    alone = {sid: _alone(sid, w, h, L, data[sid][0], *data[sid][1:]) for sid, w, h, L in cams}
+    srv = StereoServer(max_batch=3, lanes=1, reserve_bytes=0)
+    state = srv.footprint(256, 200, 3)
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    free, _ = torch.cuda.mem_get_info()
+    srv.reserve = free - int(1.5 * state)
+    for sid, w, h, L in cams:
+        fr, mask, tv, cv = data[sid]
+        srv.open_stream(sid, w, h, mask, tv, cv, L, P)
+    assert srv.counters["parks"] >= 1
+    reqs = []
+    for k in range(2):
+        for sid, _, _, _ in cams:
+            reqs.append(srv.submit(sid, *data[sid][0][k]))
+    srv.run_until_idle()
+    assert srv.counters["unparks"] >= 1 and srv.counters["deferred"] >= 1
+    for r in reqs:
+        k = [q for q in reqs if q.stream_id == r.stream_id].index(r)
+        assert np.array_equal(r.u, alone[r.stream_id][k]), (r.stream_id, k)
+
+
+def test_cancel_and_close_between_frames(gpu):
+    """A queued request can be withdrawn; a stream closed between its frames leaves the other
+    streams' results unchanged."""
+    from vfs_b200.serving import StereoServer
+    (s0, w0, h0, L0), (s1, w1, h1, L1) = CAMS[0], CAMS[1]
+    f0, m0, tv0, cv0 = _frames(s0, w0, h0, n=3)
+    f1, m1, tv1, cv1 = _frames(s1, w1, h1, n=3)
+    want0 = _alone(s0, w0, h0, L0, f0, m0, tv0, cv0)
+    srv = StereoServer(max_batch=2, lanes=2, reserve_bytes=0)
+    srv.open_stream(s0, w0, h0, m0, tv0, cv0, L0, P)
+    srv.open_stream(s1, w1, h1, m1, tv1, cv1, L1, P)
+    r0 = [srv.submit(s0, *f0[0])]
+    r1 = srv.submit(s1, *f1[0])
+    extra = srv.submit(s1, *f1[1])
+    assert srv.cancel(extra) and extra.cancelled and not srv.cancel(extra)
+    srv.run_until_idle()
+    assert r1.u is not None and extra.u is None
+    srv.close_stream(s1)
+    assert s1 not in srv.cameras
+    for a, b in f0[1:]:
+        r0.append(srv.submit(s0, a, b))
+    srv.run_until_idle()
+    for k in range(3):
+        assert np.array_equal(r0[k].u, want0[k]), k
+    assert srv.stats()["cancelled"] == 1

@@ -1,0 +1,151 @@
+"""Warm starts, whole-state export / import, and allocation failures, on the GPU."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from tests.helpers import params, random_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(i0, mask, tv, cv, p, fused, half=False):
+    from vfs_b200.stereotgv import StereoTgv
+    s = StereoTgv()
+    s.set_solve_path(fused, half)
+    s.limitRange = p["limit_range"]
+    h, w = i0.shape
+    s.initialize(w, h, p["beta"], p["gamma"], p["alpha0"], p["alpha1"], p["tsl"], p["lam"], p["n_levels"],
+                 p["f_scale"], p["n_warp"], p["n_iter"])
+    s.copyMaskToDevice(mask)
+    s.loadVectorFields(tv, cv)
+    return s
+
+
+def _frames(w, h, n, seed):
+    return [random_case(w, h, seed=seed + k)[:2] for k in range(n)]
+
+
+@pytest.mark.parametrize("masked", [True, False], ids=["masked", "plain"])
+@pytest.mark.parametrize("level", [0, 1, 2])
+def test_warm_start_fused_matches_dropin(gpu, masked, level):
+    """Warm starts from level 0, 1 and 2 (of 3): the fused FP32 path (with CUDA graphs) gives
+    the drop-in path's bits over four frames; the first frame is a cold solve."""
+    w, h = 130, 101
+    _, _, mask, tv, cv = random_case(w, h, seed=71)
+    p = params(n_levels=3, n_warp=2, n_iter=7)
+    frames = _frames(w, h, 4, seed=300)
+    a = _solver(frames[0][0], mask, tv, cv, p, fused=False)
+    b = _solver(frames[0][0], mask, tv, cv, p, fused=True)
+    c = _solver(frames[0][0], mask, tv, cv, p, fused=False)  # cold reference
+    a.set_warm_start(level)
+    b.set_warm_start(level)
+    for k, (i0, i1) in enumerate(frames):
+        for s in (a, b, c):
+            s.copyImagesToDevice(i0, i1)
+            (s.solveStereoForwardMasked if masked else s.solveStereoForward)()
+        ua, ub, uc = a.copy1DDisparityToHost(), b.copy1DDisparityToHost(), c.copy1DDisparityToHost()
+        assert np.array_equal(ua, ub), k
+        if k == 0:
+            assert np.array_equal(ua, uc)  # nothing to start from yet
+        assert np.isfinite(ua).all()
+
+
+def test_warm_start_on_a_sequence(gpu):
+    """On a synthetic camera sequence a warm start from the coarsest level stays close to the
+    cold solve of the same frame (the method's answer from zero)."""
+    from vfs_b200 import synth
+    w, h = 424, 400
+    fields, gen = synth.make_sequence(w, h, seed=5, n_frames=4)
+    frames = list(gen)
+    sp = synth.SOLVER_PARAMS
+    L = synth.n_levels_for(w)
+    p = params(beta=sp["beta"], gamma=sp["gamma"], n_levels=L, n_warp=sp["nWarpIters"], n_iter=sp["nSolverIters"],
+               limit_range=synth.LIMIT_RANGE)
+    warm = _solver(frames[0][0], fields["mask"], fields["tv"], fields["cv"], p, fused=True, half=True)
+    warm.set_warm_start(L - 1)
+    m = fields["mask"] > 0
+    for k, (i0, i1) in enumerate(frames):
+        cold = _solver(i0, fields["mask"], fields["tv"], fields["cv"], p, fused=True, half=True)
+        cold.copyImagesToDevice(i0, i1)
+        cold.solveStereoForwardMasked()
+        warm.copyImagesToDevice(i0, i1)
+        warm.solveStereoForwardMasked()
+        d = np.abs(warm.copy1DDisparityToHost() - cold.copy1DDisparityToHost())[m]
+        assert d.mean() < 0.05, (k, d.mean())
+
+
+@pytest.mark.parametrize("fused,half", [(False, False), (True, False), (True, True)], ids=["plain", "fp32", "fp16"])
+def test_export_import_continues_bit_for_bit(gpu, fused, half):
+    """Two frames on handle A, its state exported and imported into a fresh handle B (same
+    size and levels, nothing else uploaded): B's third frame equals A's."""
+    from vfs_b200.stereotgv import StereoTgv
+    w, h = 97, 71
+    _, _, mask, tv, cv = random_case(w, h, seed=81)
+    p = params(n_levels=2, n_warp=2, n_iter=5)
+    frames = _frames(w, h, 3, seed=400)
+    a = _solver(frames[0][0], mask, tv, cv, p, fused=fused, half=half)
+    a.set_warm_start(1)
+    for i0, i1 in frames[:2]:
+        a.copyImagesToDevice(i0, i1)
+        a.solveStereoForwardMasked()
+    st = a.export_state()
+    b = StereoTgv()
+    b.set_solve_path(fused, half)
+    b.limitRange = p["limit_range"]
+    b.initialize(w, h, p["beta"], p["gamma"], p["alpha0"], p["alpha1"], p["tsl"], p["lam"], p["n_levels"],
+                 p["f_scale"], p["n_warp"], p["n_iter"])
+    b.set_warm_start(1)
+    b.import_state(st)
+    for s in (a, b):
+        s.copyImagesToDevice(*frames[2])
+        s.solveStereoForwardMasked()
+    assert np.array_equal(a.copy1DDisparityToHost(), b.copy1DDisparityToHost())
+    assert np.array_equal(a.copyDisparityToHost(), b.copyDisparityToHost())
+
+
+def test_import_refuses_another_geometry(gpu):
+    from vfs_b200.stereotgv import StereoTgv, VfsError
+    _, _, mask, tv, cv = random_case(64, 48, seed=1)
+    p = params(n_levels=2, n_warp=1, n_iter=2)
+    a = _solver(np.zeros((48, 64), np.uint8), mask, tv, cv, p, fused=False)
+    st = a.export_state()
+    b = StereoTgv()
+    b.initialize(64, 50, p["beta"], p["gamma"], p["alpha0"], p["alpha1"], p["tsl"], p["lam"], 2, 2.0, 1, 2)
+    with pytest.raises(VfsError):
+        b.import_state(st)
+    with pytest.raises(VfsError):
+        b.import_state(st[:100])
+
+
+def test_allocation_failure_is_reported_and_leaks_nothing(gpu):
+    """An injected device-pool allocation failure makes initialize return VFS_ERR_NOMEM with
+    nothing left allocated, and the handle initialises normally afterwards."""
+    import torch
+    from vfs_b200._native import lib
+    from vfs_b200.stereotgv import StereoTgv, VfsError
+    L = lib()
+    s = StereoTgv()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert L.vfs_debug_fail_allocation(1) == 0
+    with pytest.raises(VfsError) as e:
+        s.initialize(424, 400, 10.0, 0.8, 17.0, 1.2, 1.0, 5.0, 4, 2.0, 1, 1)
+    assert e.value.status == -4
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 >= free0 - (2 << 20)  # nothing of the failed pool stays allocated
+    s.initialize(424, 400, 10.0, 0.8, 17.0, 1.2, 1.0, 5.0, 4, 2.0, 1, 1)
+    # the fused pool's allocation fails the same way on the first fused solve
+    s.set_solve_path(True, True)
+    _, _, mask, tv, cv = random_case(424, 400, seed=2)
+    s.copyMaskToDevice(mask)
+    s.loadVectorFields(tv, cv)
+    s.copyImagesToDevice(np.zeros((400, 424), np.uint8), np.zeros((400, 424), np.uint8))
+    assert L.vfs_debug_fail_allocation(1) == 0
+    with pytest.raises(VfsError) as e:
+        s.solveStereoForwardMasked()
+    assert e.value.status == -4
+    s.solveStereoForwardMasked()  # the retry allocates and solves
+    assert np.isfinite(s.copy1DDisparityToHost()).all()
+    assert L.vfs_debug_fail_allocation(0) == 0

@@ -1,21 +1,30 @@
 """Continuous-batching stereo server on one GPU.
 
-Camera streams are opened once. Each stream owns a solver handle whose device state
-(pyramid, vector fields, mask and the solver buffers whose stale values the reference
-carries between frames) stays on the GPU between its frames. A stream is admitted only when
-its device footprint (``vfs_estimate_device_bytes``) plus a reserve fits in the free device
-memory.
+Camera streams are opened once.  Each stream owns a solver handle whose device state (pyramid,
+vector fields, mask, the solver buffers whose stale values the reference carries between frames,
+and, with warm starts, the previous disparity) stays on the GPU between its frames.
 
-Requests (one stereo pair of a stream) queue on the host. The server runs ``lanes`` batch
-slots, each with its own CUDA stream. Whenever a slot is free it takes up to ``max_batch``
-waiting requests, at most one per camera (a camera's frames are solved in order), and
-launches them as one batched fused solve. The launch overlaps the batches already on the
-GPU. Finished slots are detected by event, their disparities copied back, and their requests'
-latencies recorded. A request therefore joins the next free slot without waiting for the
-batches in flight.
+Requests (one stereo pair of a stream) queue on the host.  The server runs ``lanes`` batch slots,
+each with its own CUDA stream.  Whenever a slot is free it takes up to ``max_batch`` waiting
+requests, at most one per camera (a camera's frames are solved in order), and launches them as
+one batched fused solve that overlaps the batches already on the GPU.  Finished slots are
+detected by event, their disparities copied back, and their requests' latencies recorded.  A
+request therefore joins the next free slot without waiting for the batches in flight.
+
+Admission by free device memory happens per request, as slots and memory free up:
+* a request is launched only when the device memory it still needs fits in the free memory
+  less ``reserve_bytes`` (its stream's state if the stream is parked, the fused buffers on a
+  stream's first fused solve, and its image and disparity buffers); otherwise it waits;
+* to make room, the server parks idle streams, least recently used first: their state is
+  exported to page-locked host memory (``vfs_export_state``) and their device memory freed;
+  a parked stream's next request brings the state back (``vfs_import_state``), and the stream
+  continues bit for bit where it stopped.
+Opening a stream allocates its state the same way (parking idle streams if needed) and is refused
+with AdmissionError when even that leaves no room; a request that cannot fit with every other
+stream parked raises AdmissionError instead of waiting for ever.
 
 Each pair's solve reads only its own state, so a stream's results are the same whether it is
-served alone or in a mix (``tests/test_gpu_serving.py``).
+served alone, in a mix, or parked in between (``tests/test_gpu_serving.py``).
 """
 from __future__ import annotations
 
@@ -31,7 +40,7 @@ from .stereotgv import StereoBatch, StereoTgv
 
 
 class AdmissionError(RuntimeError):
-    """A stream cannot be admitted: not enough free device memory."""
+    """A stream cannot be admitted: its footprint does not fit beside the reserve."""
 
 
 @dataclass
@@ -44,6 +53,7 @@ class Request:
     t_launch: float = 0.0
     t_done: float = 0.0
     u: Optional[np.ndarray] = None
+    cancelled: bool = False
 
     @property
     def latency_ms(self) -> float:
@@ -55,9 +65,18 @@ class _Camera:
     stream_id: int
     width: int
     height: int
-    solver: StereoTgv
+    n_levels: int
+    params: dict
+    mask: np.ndarray
+    tv: np.ndarray
+    cv: np.ndarray
+    warm_level: int
+    solver: Optional[StereoTgv] = None   # None while parked
+    parked_state: Optional[object] = None  # page-locked host copy of the state while parked
     busy: bool = False
     frames: int = 0
+    last_used: float = 0.0
+    fused_ready: bool = False  # its fused buffers exist (allocated on the first fused solve)
 
 
 @dataclass
@@ -69,6 +88,8 @@ class _Lane:
     ins: list = field(default_factory=list)
     outs: list = field(default_factory=list)
     hosts: list = field(default_factory=list)
+    # page-locked staging reused from batch to batch: shape -> list of (i0, i1, u) host tensors
+    pinned: Dict[tuple, list] = field(default_factory=dict)
 
     @property
     def busy(self) -> bool:
@@ -108,38 +129,128 @@ class StereoServer:
             self.lanes.append(_Lane(stream=st, batch=b))
         self.done: List[Request] = []
         self._seq = 0
+        self.counters = collections.Counter()  # deferred admissions, parks, unparks, cancels
 
-    # ---- streams --------------------------------------------------------------------
+    # ---- memory -----------------------------------------------------------------------
+    def _free(self) -> int:
+        free, _ = self.torch.cuda.mem_get_info(self.device)
+        return int(free)
+
+    def _state_bytes(self, cam: _Camera, fused: bool) -> int:
+        return int(lib().vfs_estimate_device_bytes(cam.width, cam.height, cam.n_levels, cam.params["fScale"], 32,
+                                                   1 if fused else 0))
+
+    def _request_bytes(self, cam: _Camera) -> int:
+        """Device memory a request of this camera still needs before it can run."""
+        need = 2 * cam.width * cam.height + 4 * cam.width * cam.height  # images and disparity
+        if cam.solver is None:
+            need += self._state_bytes(cam, self.path != "plain" and cam.fused_ready)
+        if self.path != "plain" and not cam.fused_ready:
+            need += self._state_bytes(cam, True) - self._state_bytes(cam, False)
+        return need
+
     def footprint(self, width: int, height: int, n_levels: int, f_scale: float = 2.0) -> int:
         return int(lib().vfs_estimate_device_bytes(width, height, n_levels, f_scale, 32, 1))
 
+    # ---- streams --------------------------------------------------------------------
     def open_stream(self, stream_id: int, width: int, height: int, mask, tv, cv, n_levels: int,
-                    params: Optional[dict] = None) -> None:
-        """Admit a camera stream: allocate its handle if its footprint fits in free memory."""
+                    params: Optional[dict] = None, warm_start_level: int = -1) -> None:
+        """Admit a camera stream and allocate its state, parking idle streams if that makes
+        room.  warm_start_level >= 0: each frame after the first starts from the previous
+        disparity at that pyramid level (vfs_set_warm_start)."""
         if stream_id in self.cameras:
             raise ValueError(f"stream {stream_id} already open")
         p = dict(DEFAULT_PARAMS, **(params or {}))
-        need = int(lib().vfs_estimate_device_bytes(width, height, n_levels, p["fScale"], 32,
-                                                   0 if self.path == "plain" else 1))
-        free, _ = self.torch.cuda.mem_get_info(self.device)
-        if need == 0 or need + self.reserve > free:
-            raise AdmissionError(f"stream {stream_id}: needs {need} bytes + reserve {self.reserve}, free {free}")
+        cam = _Camera(stream_id, width, height, n_levels, p, np.ascontiguousarray(mask, np.float32),
+                      np.ascontiguousarray(tv, np.float32), np.ascontiguousarray(cv, np.float32), int(warm_start_level))
+        need = self._state_bytes(cam, False)
+        if need == 0:
+            raise AdmissionError(f"stream {stream_id}: invalid geometry")
+        if not self._ensure_room(need, keep=set()):
+            raise AdmissionError(f"stream {stream_id}: needs {need} bytes + reserve {self.reserve}, "
+                                 f"free {self._free()}")
+        cam.solver = self._new_solver(cam)
+        cam.solver.copyMaskToDevice(cam.mask)
+        cam.solver.loadVectorFields(cam.tv, cam.cv)
+        cam.last_used = time.perf_counter()
+        self.cameras[stream_id] = cam
+
+    def _new_solver(self, cam: _Camera) -> StereoTgv:
+        p = cam.params
         s = StereoTgv()
         s.set_solve_path(self.path != "plain", self.half)
         s.limitRange = p["limitRange"]
-        s.initialize(width, height, p["beta"], p["gamma"], p["alpha0"], p["alpha1"], p["timestep_lambda"],
-                     p["lambda_"], n_levels, p["fScale"], p["nWarpIters"], p["nSolverIters"])
-        s.copyMaskToDevice(mask)
-        s.loadVectorFields(tv, cv)
-        self.cameras[stream_id] = _Camera(stream_id, width, height, s)
+        s.initialize(cam.width, cam.height, p["beta"], p["gamma"], p["alpha0"], p["alpha1"], p["timestep_lambda"],
+                     p["lambda_"], cam.n_levels, p["fScale"], p["nWarpIters"], p["nSolverIters"])
+        if cam.warm_level >= 0:
+            s.set_warm_start(cam.warm_level)
+        return s
+
+    def _release_solver(self, cam: _Camera) -> None:
+        for lane in self.lanes:  # idle batches still list their last members
+            if not lane.busy:
+                lane.batch.clear()
+        cam.solver.close()
+        cam.solver = None
+
+    def park_stream(self, stream_id: int) -> None:
+        """Move an idle stream's state to page-locked host memory and free its device memory."""
+        cam = self.cameras[stream_id]
+        if cam.solver is None:
+            return
+        if cam.busy:
+            raise RuntimeError(f"stream {stream_id} has a frame in flight")
+        n = int(lib().vfs_state_bytes(cam.solver.handle))
+        host = self.torch.empty(n, dtype=self.torch.uint8).pin_memory()
+        st = lib().vfs_export_state(cam.solver.handle, host.data_ptr(), n)
+        if st != 0:
+            raise RuntimeError(f"stream {stream_id}: export failed ({st})")
+        cam.parked_state = host
+        self._release_solver(cam)
+        self.counters["parks"] += 1
+
+    def _unpark(self, cam: _Camera) -> None:
+        s = self._new_solver(cam)
+        host = cam.parked_state
+        st = lib().vfs_import_state(s.handle, host.data_ptr(), host.numel())
+        if st != 0:
+            s.close()
+            raise RuntimeError(f"stream {cam.stream_id}: import failed ({st})")
+        cam.solver = s
+        cam.parked_state = None
+        self.counters["unparks"] += 1
+
+    def _ensure_room(self, need: int, keep: set) -> bool:
+        """Park idle streams (least recently used first, those with waiting requests last)
+        until `need` bytes fit beside the reserve."""
+        if need + self.reserve <= self._free():
+            return True
+        self.torch.cuda.empty_cache()  # memory torch keeps cached is not free to the driver
+        if need + self.reserve <= self._free():
+            return True
+        waiting = {r.stream_id for r in self.queue}
+        idle = [c for c in self.cameras.values()
+                if c.solver is not None and not c.busy and c.stream_id not in keep]
+        idle.sort(key=lambda c: (c.stream_id in waiting, c.last_used))
+        for c in idle:
+            self.park_stream(c.stream_id)
+            self.torch.cuda.synchronize(self.device)
+            if need + self.reserve <= self._free():
+                return True
+        return need + self.reserve <= self._free()
 
     def close_stream(self, stream_id: int) -> None:
+        """Close a stream between its frames; its waiting requests are cancelled."""
         cam = self.cameras.get(stream_id)
         if cam is None:
             return
         if cam.busy:
             raise RuntimeError(f"stream {stream_id} has a frame in flight")
-        cam.solver.synchronize()
+        for r in [r for r in self.queue if r.stream_id == stream_id]:
+            self.cancel(r)
+        if cam.solver is not None:
+            cam.solver.synchronize()
+            self._release_solver(cam)
         del self.cameras[stream_id]
 
     # ---- requests -------------------------------------------------------------------
@@ -150,6 +261,16 @@ class StereoServer:
         self._seq += 1
         self.queue.append(r)
         return r
+
+    def cancel(self, request: Request) -> bool:
+        """Withdraw a request that has not been launched yet; False if it already runs or ran."""
+        try:
+            self.queue.remove(request)
+        except ValueError:
+            return False
+        request.cancelled = True
+        self.counters["cancelled"] += 1
+        return True
 
     def pending(self) -> int:
         return len(self.queue) + sum(len(l.requests) for l in self.lanes)
@@ -162,44 +283,74 @@ class StereoServer:
                 for r, h in zip(lane.requests, lane.hosts):
                     r.u = h.numpy().copy()
                     r.t_done = now
-                    cam = self.cameras[r.stream_id]
-                    cam.busy = False
-                    cam.frames += 1
+                    cam = self.cameras.get(r.stream_id)
+                    if cam is not None:
+                        cam.busy = False
+                        cam.frames += 1
+                        cam.last_used = now
                     fin.append(r)
                 lane.event = None
                 lane.requests, lane.ins, lane.outs, lane.hosts = [], [], [], []
         self.done.extend(fin)
         return fin
 
-    def _launch(self, lane: _Lane) -> bool:
-        torch = self.torch
-        picked, seen = [], set()
-        rest = collections.deque()
-        while self.queue and len(picked) < self.max_batch:
-            r = self.queue.popleft()
+    def _admit(self) -> List[Request]:
+        """Pick up to max_batch waiting requests (one per camera, in arrival order) whose device
+        memory fits, parking idle streams to make room; the others keep waiting."""
+        picked, seen, committed = [], set(), 0
+        for r in list(self.queue):
+            if len(picked) >= self.max_batch:
+                break
             cam = self.cameras[r.stream_id]
             if cam.busy or r.stream_id in seen:
-                rest.append(r)  # a camera's frames run in order: at most one in flight
+                continue  # a camera's frames run in order: at most one in flight
+            need = self._request_bytes(cam)
+            if not self._ensure_room(committed + need, keep=seen | {r.stream_id}):
+                self.counters["deferred"] += 1
                 continue
+            if cam.solver is None:
+                self._unpark(cam)
+                need = self._request_bytes(cam)  # the state is resident now
+            committed += need
             picked.append(r)
             seen.add(r.stream_id)
-        rest.extend(self.queue)
-        self.queue = rest
+        for r in picked:
+            self.queue.remove(r)
+        return picked
+
+    def _staging(self, lane: _Lane, h: int, w: int, k: int):
+        """The k-th page-locked (i0, i1, u) staging set of a lane for h x w frames."""
+        pool = lane.pinned.setdefault((h, w), [])
+        torch = self.torch
+        while len(pool) <= k:
+            pool.append((torch.empty((h, w), dtype=torch.uint8).pin_memory(),
+                         torch.empty((h, w), dtype=torch.uint8).pin_memory(),
+                         torch.empty((h, w), dtype=torch.float32).pin_memory()))
+        return pool[k]
+
+    def _launch(self, lane: _Lane) -> bool:
+        torch = self.torch
+        picked = self._admit()
         if not picked:
             return False
         st = lane.stream
         lane.batch.clear()
         now = time.perf_counter()
+        used = collections.Counter()
         with torch.cuda.stream(st):
-            ins, outs = [], []
+            ins, outs, hosts = [], [], []
             for r in picked:
                 cam = self.cameras[r.stream_id]
                 cam.busy = True
                 cam.solver.set_stream(st)
-                a = torch.from_numpy(np.ascontiguousarray(r.i0)).pin_memory().to(self.device, non_blocking=True)
-                b = torch.from_numpy(np.ascontiguousarray(r.i1)).pin_memory().to(self.device, non_blocking=True)
-                ins.append((a, b))
+                key = (cam.height, cam.width)
+                hi0, hi1, hu = self._staging(lane, cam.height, cam.width, used[key])
+                used[key] += 1
+                np.copyto(hi0.numpy(), r.i0)
+                np.copyto(hi1.numpy(), r.i1)
+                ins.append((hi0.to(self.device, non_blocking=True), hi1.to(self.device, non_blocking=True)))
                 outs.append(torch.empty((cam.height, cam.width), dtype=torch.float32, device=self.device))
+                hosts.append(hu)
                 if self.path != "plain":
                     lane.batch.add(cam.solver)
                 r.t_launch = now
@@ -211,14 +362,13 @@ class StereoServer:
             else:
                 # each request's copies and solve on its own lane of the batch
                 lane.batch.solve_device(ins, outs)
-            for out in outs:
-                host = torch.empty(out.shape, dtype=torch.float32, pin_memory=True)
-                host.copy_(out, non_blocking=True)
-                lane.outs.append(out)
-                lane.hosts.append(host)
-            lane.ins = ins  # kept alive until the batch completes
+            for out, hu in zip(outs, hosts):
+                hu.copy_(out, non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(st)
+        for r in picked:
+            self.cameras[r.stream_id].fused_ready = self.path != "plain"
+        lane.ins, lane.outs, lane.hosts = ins, outs, hosts  # kept alive until the batch completes
         lane.event = ev
         lane.requests = picked
         return True
@@ -226,9 +376,15 @@ class StereoServer:
     def step(self) -> List[Request]:
         """One scheduling pass: collect finished batches, launch waiting requests on free slots."""
         fin = self._harvest()
+        launched = False
         for lane in self.lanes:
             if not lane.busy and self.queue:
-                self._launch(lane)
+                launched = self._launch(lane) or launched
+        if self.queue and not launched and not any(l.busy for l in self.lanes):
+            # nothing runs and nothing could be admitted: no memory will free up by waiting
+            r = self.queue[0]
+            raise AdmissionError(f"request {r.seq} of stream {r.stream_id} does not fit in free device memory "
+                                 f"beside the reserve even with every other stream parked")
         return fin
 
     def run_until_idle(self, poll_s: float = 0.0002) -> None:
@@ -240,13 +396,16 @@ class StereoServer:
     # ---- statistics -----------------------------------------------------------------
     def stats(self, since: float = 0.0) -> dict:
         d = [r for r in self.done if r.t_submit >= since]
+        out = {k: int(v) for k, v in self.counters.items()}
         if not d:
-            return {"frames": 0}
+            out["frames"] = 0
+            return out
         lat = np.array([r.latency_ms for r in d])
         span = max(r.t_done for r in d) - min(r.t_submit for r in d)
-        return {"frames": len(d), "frames_per_s": len(d) / span if span > 0 else None,
-                "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                "mean_ms": float(lat.mean())}
+        out.update({"frames": len(d), "frames_per_s": len(d) / span if span > 0 else None,
+                    "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                    "mean_ms": float(lat.mean())})
+        return out
 
 
 def poisson_schedule(rates: Dict[int, float], n_frames: Dict[int, int], seed: int = 0):

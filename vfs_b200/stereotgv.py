@@ -48,14 +48,18 @@ class StereoTgv:
         self.width = self.height = 0
         self._stream = None
 
-    def __del__(self):
+    def close(self) -> None:
+        """Destroy the handle now (frees its device memory); the object is unusable after."""
         h = getattr(self, "_h", None)
         if h:
-            try:
-                self._L.vfs_destroy(h)
-            except Exception:
-                pass
+            self._L.vfs_destroy(h)
             self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     @property
     def handle(self):
