@@ -73,6 +73,11 @@ int vfs_set_camera(vfs_stereo* s, float baseline, float focal);
  * point.  initialize and loadVectorFields forget the previous frame. */
 int vfs_set_warm_start(vfs_stereo* s, int level);
 
+/* Number of CUDA graph executables a handle's fused solves keep cached (no counterpart in the
+ * reference).  Graphs captured for an older mask or initialize are destroyed on the next
+ * solve, and at most 64 are kept (vfs_batch_cached_graphs: the same for a batch). */
+int vfs_cached_graphs(const vfs_stereo* s);
+
 /* Whole-state export / import (no counterpart in the reference): the handle's device state
  * (image pyramid, mask, fields, every solver buffer with the stale values the reference keeps
  * between frames, and the warm-start disparity), so that a handle initialised with the same
@@ -164,6 +169,7 @@ size_t vfs_estimate_device_bytes(int width, int height, int nLevels, float fScal
 #define VFS_BATCH_MAX 24
 typedef struct vfs_batch vfs_batch;
 int vfs_batch_create(vfs_batch** out);
+int vfs_batch_cached_graphs(const vfs_batch* b);
 int vfs_batch_destroy(vfs_batch* b);
 const char* vfs_batch_last_error(const vfs_batch* b);
 int vfs_batch_set_stream(vfs_batch* b, void* cuda_stream);

@@ -149,3 +149,87 @@ def test_allocation_failure_is_reported_and_leaks_nothing(gpu):
     s.solveStereoForwardMasked()  # the retry allocates and solves
     assert np.isfinite(s.copy1DDisparityToHost()).all()
     assert L.vfs_debug_fail_allocation(0) == 0
+
+
+def test_graph_cache_drops_graphs_of_old_masks(gpu):
+    """Every new mask renews the handle's generation; the graphs captured under the old one are
+    destroyed on the next solve instead of accumulating."""
+    from vfs_b200._native import lib
+    w, h = 96, 64
+    i0, i1, mask, tv, cv = random_case(w, h, seed=90)
+    p = params(n_levels=2, n_warp=1, n_iter=3)
+    s = _solver(i0, mask, tv, cv, p, fused=True, half=True)
+    counts = []
+    for k in range(6):
+        m = mask.copy()
+        m[:, : 2 + k] = 0  # a different mask each time
+        s.copyMaskToDevice(m)
+        for _ in range(2):  # both pointer states of the solve
+            s.copyImagesToDevice(i0, i1)
+            s.solveStereoForwardMasked()
+        counts.append(lib().vfs_cached_graphs(s.handle))
+    assert max(counts) <= 4, counts
+
+
+def test_cpp_dropin_header_solves_on_the_gpu(gpu, tmp_path):
+    """A program written against include/stereotgv.h (the reference's class) solves a pair on
+    the GPU and gets the same disparity as the Python binding of the same library."""
+    import os
+    import subprocess
+    from vfs_b200.build import LIB
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    w, h = 96, 64
+    i0, i1, mask, tv, cv = random_case(w, h, seed=77)
+    p = params(n_levels=2, n_warp=2, n_iter=6)
+    for name, arr in (("i0", i0), ("i1", i1), ("mask", mask.astype(np.float32)), ("tv", tv.astype(np.float32)),
+                      ("cv", cv.astype(np.float32))):
+        arr.tofile(str(tmp_path / f"{name}.bin"))
+    src = tmp_path / "solve.cpp"
+    src.write_text(r"""
+#include "stereotgv.h"
+#include <cstdio>
+#include <vector>
+template <class T> static std::vector<T> load(const char* dir, const char* name, size_t n) {
+  std::vector<T> v(n);
+  char path[512];
+  std::snprintf(path, sizeof(path), "%s/%s.bin", dir, name);
+  FILE* f = std::fopen(path, "rb");
+  if (!f || std::fread(v.data(), sizeof(T), n, f) != n) { std::printf("read %s failed\n", path); std::exit(3); }
+  std::fclose(f);
+  return v;
+}
+int main(int argc, char** argv) {
+  const int W = 96, H = 64;
+  const char* dir = argv[1];
+  auto i0 = load<unsigned char>(dir, "i0", W * H), i1 = load<unsigned char>(dir, "i1", W * H);
+  auto mask = load<float>(dir, "mask", W * H);
+  auto tv = load<float>(dir, "tv", 2 * W * H), cv = load<float>(dir, "cv", 2 * W * H);
+  StereoTgv s;                      // the reference's class and call sequence
+  s.limitRange = 0.1f;
+  int st = s.initialize(W, H, 10.0f, 0.8f, 17.0f, 1.2f, 1.0f, 5.0f, 2, 2.0f, 2, 6);
+  if (!st) st = s.copyMaskToDevice(mask.data());
+  if (!st) st = s.loadVectorFields(tv.data(), cv.data());
+  if (!st) st = s.copyImagesToDevice(i0.data(), i1.data());
+  if (!st) st = s.solveStereoForwardMasked();
+  std::vector<float> u(W * H);
+  if (!st) st = s.copy1DDisparityToHost(u.data());
+  if (st) { std::printf("status %d\n", st); return 2; }
+  char path[512];
+  std::snprintf(path, sizeof(path), "%s/u.bin", dir);
+  FILE* f = std::fopen(path, "wb");
+  std::fwrite(u.data(), sizeof(float), u.size(), f);
+  std::fclose(f);
+  return 0;
+}
+""")
+    exe = tmp_path / "solve"
+    libdir = os.path.dirname(LIB)
+    r = subprocess.run(["g++", "-std=c++17", f"-I{os.path.join(root, 'include')}", str(src), "-o", str(exe),
+                        f"-L{libdir}", "-lvfs_b200", f"-Wl,-rpath,{libdir}"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe), str(tmp_path)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    u_cpp = np.fromfile(str(tmp_path / "u.bin"), np.float32).reshape(h, w)
+    from tests.helpers import run_gpu
+    u_py = run_gpu(i0, i1, mask, tv, cv, p, True).copy1DDisparityToHost()
+    assert np.array_equal(u_cpp, u_py)

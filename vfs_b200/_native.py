@@ -46,6 +46,8 @@ SIGNATURES = {
     "vfs_set_camera": [_vp, _f, _f],
     "vfs_set_tensor_math": [_vp, _i],
     "vfs_set_warm_start": [_vp, _i],
+    "vfs_cached_graphs": [_vp],
+    "vfs_batch_cached_graphs": [_vp],
     "vfs_state_bytes": [_vp],
     "vfs_export_state": [_vp, _vp, _sz],
     "vfs_import_state": [_vp, _vp, _sz],

@@ -511,6 +511,36 @@ void FusedEngine::clear() {
   cache_.clear();
 }
 
+// An executable still in flight is freed when it completes (cudaGraphExecDestroy), and so are
+// recorded events (cudaEventDestroy).
+void FusedEngine::drop(std::map<std::vector<uintptr_t>, Entry>::iterator it) {
+  if (it->second.exec) cudaGraphExecDestroy(it->second.exec);
+  for (auto e : it->second.events) cudaEventDestroy(e);
+  cache_.erase(it);
+}
+
+void FusedEngine::evict(const std::vector<StereoTgvImpl*>& pairs) {
+  for (auto it = cache_.begin(); it != cache_.end();) {
+    bool stale = false;
+    for (const auto& o : it->second.owners)
+      for (const auto* s : pairs)
+        if (o.first == s && o.second != s->generation) stale = true;
+    if (stale) {
+      auto next = std::next(it);
+      drop(it);
+      it = next;
+    } else {
+      ++it;
+    }
+  }
+  while (cache_.size() >= kMaxGraphs) {
+    auto lru = cache_.begin();
+    for (auto it = cache_.begin(); it != cache_.end(); ++it)
+      if (it->second.last_use < lru->second.last_use) lru = it;
+    drop(lru);
+  }
+}
+
 void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
   for (auto* s : pairs) {
     if (!s->initialized()) throw ArgError{"fused solve: pair not initialized"};
@@ -664,7 +694,9 @@ void FusedEngine::solve_parts(std::vector<StereoTgvImpl*>& pairs, bool masked, b
   }
   auto it = cache_.find(key);
   if (it == cache_.end()) {
+    evict(pairs);
     Entry e;
+    for (auto* s : pairs) e.owners.emplace_back(s, s->generation);
     std::vector<ProfRec> saved = prof->profRecords();
     prof->profReset();
     prof->capture_events = &e.events;
@@ -695,6 +727,7 @@ void FusedEngine::solve_parts(std::vector<StereoTgvImpl*>& pairs, bool masked, b
     for (size_t k = 0; k < pairs.size(); k++) set_ptrs(pairs[k], before[k]);
     it = cache_.emplace(key, std::move(e)).first;
   }
+  it->second.last_use = ++use_clock_;
   VFS_CUDA(cudaGraphLaunch(it->second.exec, st));
   launch_counter().fetch_add(it->second.kernels);
   for (size_t k = 0; k < pairs.size(); k++) set_ptrs(pairs[k], it->second.after[k]);

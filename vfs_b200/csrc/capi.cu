@@ -170,6 +170,9 @@ int vfs_set_limit_range(vfs_stereo* s, float lr) {
   });
 }
 
+int vfs_cached_graphs(const vfs_stereo* s) { return s ? (int)s->impl.engine.graphs() : VFS_ERR_ARG; }
+int vfs_batch_cached_graphs(const vfs_batch* b) { return b ? (int)b->engine.graphs() : VFS_ERR_ARG; }
+
 int vfs_set_warm_start(vfs_stereo* s, int level) {
   return guarded(s, [&] {
     if (level < -1) throw vfs::ArgError{"vfs_set_warm_start: level must be -1 (off) or >= 0"};

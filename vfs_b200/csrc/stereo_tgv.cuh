@@ -71,7 +71,17 @@ class FusedEngine {
     std::vector<PairPtrs> after;
     std::vector<ProfRec> prof;
     std::vector<cudaEvent_t> events;
+    std::vector<std::pair<const StereoTgvImpl*, uint64_t>> owners;  // pairs and their generation
+    uint64_t last_use = 0;
   };
+  // Graphs of a pair captured under an older generation (an earlier mask, initialize or state
+  // import) are destroyed when the pair is next solved, and at most kMaxGraphs are kept (the
+  // least recently replayed go first), so a long-running server whose batch compositions keep
+  // changing holds a bounded number of graph executables.
+  static constexpr size_t kMaxGraphs = 64;
+  void evict(const std::vector<StereoTgvImpl*>& pairs);
+  void drop(std::map<std::vector<uintptr_t>, Entry>::iterator it);
+  uint64_t use_clock_ = 0;
   std::map<std::vector<uintptr_t>, Entry> cache_;
   std::map<std::vector<int>, std::vector<int>> tuned_;
 };
