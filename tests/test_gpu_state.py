@@ -188,6 +188,7 @@ def test_cpp_dropin_header_solves_on_the_gpu(gpu, tmp_path):
     src.write_text(r"""
 #include "stereotgv.h"
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 template <class T> static std::vector<T> load(const char* dir, const char* name, size_t n) {
   std::vector<T> v(n);
