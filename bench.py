@@ -558,6 +558,7 @@ def run_ours(args, rank, world, local):
                                                             "max_abs_vs_plain_px", "config")}
             srv = run_serving(args, emit=False)
             result["serving"] = dict(srv["serving"], config=srv["config"])
+            result["warm_start"] = warm_start_report(args.seed)
         print(json.dumps(result), flush=True)
     if world > 1:
         torch.distributed.barrier()
@@ -651,6 +652,47 @@ def run_mixed(args, emit=True):
     if emit:
         print(json.dumps(line), flush=True)
     return line
+
+
+def warm_start_report(seed, n_frames=8, width=424, height=400):
+    """Warm starts on a camera sequence with ground truth: mean |u - true disparity| inside the
+    mask (where the true disparity is finite), and the GPU time per frame, for cold solves and
+    for warm starts from the coarsest level and from two levels below it (those levels are
+    skipped).  Fused path, FP16 storage; one stream of width x height."""
+    import torch
+    from vfs_b200 import synth
+    from vfs_b200.stereotgv import StereoTgv
+    fields, gen = synth.make_sequence(width, height, seed, n_frames, with_depth=True)
+    frames = list(gen)
+    sp = synth.SOLVER_PARAMS
+    L = synth.n_levels_for(width)
+    m = fields["mask"] > 0
+    out = {"workload": f"one {width}x{height} stream, {n_frames} frames (<= 5 cm and 3 degrees per frame), "
+                       "fused FP16; error inside the mask against the disparity the rendered depth implies"}
+    for label, level in (("cold", -1), ("warm_full_pyramid", L - 1), ("warm_skip_2_levels", max(0, L - 3))):
+        s = StereoTgv()
+        s.set_solve_path(True, True)
+        s.limitRange = synth.LIMIT_RANGE
+        s.initialize(width, height, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"],
+                     sp["lambda_"], L, sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+        s.copyMaskToDevice(fields["mask"])
+        s.loadVectorFields(fields["tv"], fields["cv"])
+        s.set_warm_start(level)
+        errs, ms = [], []
+        for k, (i0, i1, depth) in enumerate(frames):
+            s.copyImagesToDevice(i0, i1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            s.solveStereoForwardMasked()
+            s.synchronize()
+            ms.append(1000 * (time.perf_counter() - t0))
+            ut = synth.true_disparity(width, height, depth)
+            ok = m & np.isfinite(ut)
+            errs.append(float(np.abs(s.copy1DDisparityToHost() - ut)[ok].mean()))
+        out[label] = {"start_level": level, "mean_abs_err_px_per_frame": errs,
+                      "mean_abs_err_px_after_first": float(np.mean(errs[1:])),
+                      "ms_per_frame_after_first": float(np.median(ms[2:] if len(ms) > 2 else ms))}
+    return out
 
 
 def run_serving(args, emit=True):

@@ -70,8 +70,8 @@ def test_serving_float_storage_matches_dropin_path(gpu):
 def test_admission_refuses_streams_that_do_not_fit(gpu):
     import torch
     from vfs_b200.serving import AdmissionError, StereoServer
-    free, _ = torch.cuda.mem_get_info()
-    srv = StereoServer(max_batch=2, lanes=1, reserve_bytes=free)  # nothing fits beside the reserve
+    _, total = torch.cuda.mem_get_info()
+    srv = StereoServer(max_batch=2, lanes=1, reserve_bytes=total)  # nothing fits beside the reserve
     fr, mask, tv, cv = _frames(0, 96, 80, n=1)
     with pytest.raises(AdmissionError):
         srv.open_stream(0, 96, 80, mask, tv, cv, 2, P)

@@ -687,6 +687,7 @@ void FusedEngine::solve_parts(std::vector<StereoTgvImpl*>& pairs, bool masked, b
     key.push_back((uintptr_t)s);
     key.push_back((uintptr_t)s->generation);
     key.push_back((uintptr_t)s->topLevel());
+    key.push_back((uintptr_t)s->warmStart());  // a warm start from the coarsest level has the cold top
     key.insert(key.end(), w, w + sizeof(PairPtrs) / sizeof(uintptr_t));
     uint32_t lr;
     std::memcpy(&lr, &s->P.limitRange, 4);

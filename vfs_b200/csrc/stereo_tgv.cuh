@@ -130,6 +130,7 @@ class StereoTgvImpl {
   // above it are skipped.
   int warm_level = -1;
   bool have_prev = false;  // d_u holds the disparity of the last solved frame (full resolution)
+  bool warmStart() const { return warm_level >= 0 && have_prev; }
   int topLevel() const {
     return (warm_level >= 0 && have_prev) ? std::min(warm_level, levels() - 1) : levels() - 1;
   }

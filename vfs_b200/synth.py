@@ -168,11 +168,25 @@ def make_pair(width: int, height: int, seed: int, baseline: float = 0.064, max_r
                       cv=calibration_field(cam, cam, R01), depth=depth, seed=seed)
 
 
+def true_disparity(width: int, height: int, depth: np.ndarray, baseline: float = 0.064) -> np.ndarray:
+    """The disparity camera 0's depth map implies along the translation field: pixel p sees the
+    point depth(p) * ray(p); the calibrated second camera, displaced by `baseline` along x, sees
+    it at p'; the disparity is (p' - p) . tv(p).  NaN where the depth is not finite."""
+    cam = EquidistantCamera(width, height)
+    b = np.array([baseline, 0.0, 0.0])
+    tv = translation_field(cam, b)
+    yy, xx = np.mgrid[0:height, 0:width].astype(np.float64)
+    X = np.asarray(depth, np.float64)[..., None] * cam.unproject(xx, yy)
+    u1, v1 = cam.project(X - b)
+    return (u1 - xx) * tv[..., 0] + (v1 - yy) * tv[..., 1]
+
+
 def make_sequence(width: int, height: int, seed: int, n_frames: int, max_step_m: float = 0.05,
                   max_step_deg: float = 3.0, baseline: float = 0.064, max_rot_deg: float = 2.0,
-                  fov_deg: float = 163.0):
+                  fov_deg: float = 163.0, with_depth: bool = False):
     """A camera stream: a fixed seeded scene and a smooth random rig trajectory (<= max_step_m
-    and <= max_step_deg per frame).  Returns (fields dict, generator of (i0, i1) frames)."""
+    and <= max_step_deg per frame).  Returns (fields dict, generator of (i0, i1) frames, or of
+    (i0, i1, depth of camera 0) with with_depth)."""
     rng = np.random.default_rng(seed)
     scene = Scene.random(rng, seed)
     cam = EquidistantCamera(width, height)
@@ -186,9 +200,9 @@ def make_sequence(width: int, height: int, seed: int, n_frames: int, max_step_m:
         vel = rng.normal(size=3)
         vel *= max_step_m * 0.7 / np.linalg.norm(vel)
         for _ in range(n_frames):
-            i0, _ = render(scene, cam, R, C, rng)
+            i0, d0 = render(scene, cam, R, C, rng)
             i1, _ = render(scene, cam, R @ R01, C + R @ b, rng)
-            yield i0, i1
+            yield (i0, i1, d0) if with_depth else (i0, i1)
             acc = rng.normal(size=3) * max_step_m * 0.2
             vel = vel + acc
             nv = np.linalg.norm(vel)
