@@ -223,19 +223,19 @@ int vfs_batch_set_fine_concurrency(vfs_batch* b, int max_pairs);
 int vfs_batch_set_pipeline(vfs_batch* b, int stagger_coarse, int priority);
 int vfs_set_autotune(vfs_stereo* s, int on);
 /* Force one variant of the fused iteration kernel at every pyramid level (-1: the tuned or
- * default choice).  0-2: 32 x (4, 8, 16 + 1)-thread blocks exchanging the west / north
- * neighbours' T p and q through shared memory; 3-5: one warp per 31-column strip of 8, 16
- * or 32 rows, neighbours by warp shuffle and registers; 6-9: several iterations per launch
- * with the tile's region held in shared memory (6: 3 iterations on 64 x 24 tiles, 7: 5 on
- * 32 x 24, 8: 3 on 23 x 23, 9: 5 on 17 x 17, 12: 7 on 11 x 11, 13: 9 on 5 x 5); 10-11: two
- * horizontally adjacent pixels per thread on 62 x 8 / 62 x 4 tiles; 14-15: the whole level in
- * the shared memory of a thread-block cluster of 16 / 8 CTAs, up to 64 iterations per launch
- * (levels whose state fits: about 3200 pixels per CTA with half storage), two cluster
- * barriers per iteration; 16-17: the same with one cluster barrier per iteration.  6-17 apply
- * to one-pair launches (other launches, and levels where they do not apply, use variant 1).
- * Every variant gives the same results; this selects speed only.  (No counterpart in the
+ * default choice).  0-2, 19: 32 x (TH + 1)-thread blocks, TH = 4, 8, 16, 15, exchanging
+ * the west / north neighbours' T p and q through shared memory; 6-9: several iterations per
+ * launch with the tile's region held in shared memory (6: 3 iterations on 64 x 24 tiles, 7: 5
+ * on 32 x 24, 8: 3 on 23 x 23, 9: 5 on 17 x 17, 12: 7 on 11 x 11, 13: 9 on 5 x 5); 14-15: the
+ * whole level in the shared memory of a thread-block cluster of 16 / 8 CTAs, up to 64
+ * iterations per launch (levels whose state fits: about 3200 pixels per CTA with half
+ * storage), two cluster barriers per iteration; 18: the 8-row tiles of variant 1 with the
+ * block's region of every input plane brought into shared memory by bulk tensor copies.
+ * 6-18 apply to one-pair launches (other launches, and levels where they do not apply, use
+ * variant 1).  3-5, 10, 11, 16 and 17 are retired and rejected with VFS_ERR_ARG.  Every
+ * variant gives the same results; this selects speed only.  (No counterpart in the
  * reference.) */
-#define VFS_ITER_VARIANTS 18
+#define VFS_ITER_VARIANTS 20
 int vfs_set_iteration_variant(vfs_stereo* s, int variant);
 /* Force one variant per pyramid level (finest first; levels beyond n_levels use variant 1),
  * e.g. to pin a tuned choice; n_levels = 0 clears it. */

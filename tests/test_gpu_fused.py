@@ -16,7 +16,7 @@ OUT = (("u", 1), ("u_", 1), ("warpUV", 2), ("i1warp", 1), ("Iu", 1), ("Iz", 1), 
 
 
 # the iteration-kernel variants that exist (3-5, 10-11 and 16-17 were removed)
-VARIANTS = (0, 1, 2, 6, 7, 8, 9, 12, 13, 14, 15, 18)
+VARIANTS = (0, 1, 2, 6, 7, 8, 9, 12, 13, 14, 15, 18, 19)
 
 def make(i0, i1, mask, tv, cv, p, fused, half=False, graph=True):
     from vfs_b200.stereotgv import StereoTgv
@@ -274,7 +274,7 @@ def test_retired_variants_are_rejected(gpu):
     from vfs_b200.stereotgv import VfsError
     i0, i1, mask, tv, cv = random_case(64, 48, seed=9)
     s = make(i0, i1, mask, tv, cv, params(n_levels=1, n_warp=1, n_iter=1), fused=True)
-    for v in (3, 4, 5, 10, 11, 16, 17, 19, -2):
+    for v in (3, 4, 5, 10, 11, 16, 17, 20, -2):
         with pytest.raises(VfsError):
             s.set_iteration_variant(v)
     s.set_iteration_variant(-1)  # back to the tuner
@@ -382,10 +382,11 @@ def test_batch_solve_device_matches_host_buffers(gpu):
 
 
 @pytest.mark.parametrize("half", [False, True], ids=["fp32", "fp16"])
-def test_tma_iteration_matches_default_at_full_size(gpu, half):
-    """The TMA-staged iteration kernel (variant 18) on a synthetic 848 x 800 fisheye pair, every
-    level: the bits of the default variant (and, with float storage, of the drop-in path); the
-    kernel's bounded copy waits never ran out."""
+def test_tma_and_15_row_iterations_match_default_at_full_size(gpu, half):
+    """The TMA-staged iteration kernel (variant 18) and the 15-row tiles (variant 19) on a
+    synthetic 848 x 800 fisheye pair, every level, with their per-row tile spans: the bits of
+    the default variant (and, with float storage, of the drop-in path); the TMA kernel's
+    bounded copy waits never ran out."""
     import ctypes
     from vfs_b200 import synth
     from vfs_b200._native import lib
@@ -394,12 +395,13 @@ def test_tma_iteration_matches_default_at_full_size(gpu, half):
     p = params(beta=sp["beta"], gamma=sp["gamma"], n_levels=synth.n_levels_for(848), n_warp=sp["nWarpIters"],
                n_iter=sp["nSolverIters"], limit_range=synth.LIMIT_RANGE)
     out = {}
-    for v in (1, 18):
+    for v in (1, 18, 19):
         s = make(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, fused=True, half=half)
         s.set_iteration_variant(v)
         solve_frames(s, pair.i0, pair.i1, True, 2)
         out[v] = (s.copy1DDisparityToHost(), s.debug_buffer("warpUV", 2))
         assert s.iteration_variants() == [v] * synth.n_levels_for(848)
-    assert np.array_equal(out[1][0], out[18][0]) and np.array_equal(out[1][1], out[18][1])
+    for v in (18, 19):
+        assert np.array_equal(out[1][0], out[v][0]) and np.array_equal(out[1][1], out[v][1]), v
     st = ctypes.c_int(-1)
     assert lib().vfs_device_status(ctypes.byref(st)) == 0 and st.value == 0

@@ -216,8 +216,8 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         A.npairs = na;
         A.span_rows = 0;
         // the TMA variant has the 8-row tiles of variant 1, and its tile spans
-        const int sv = variant == kIterTmaVariant ? 1 : variant;
-        if (na == 1 && masked && sv >= 0 && sv < 3) {
+        const int sv = variant == kIterTmaVariant ? 1 : iter_span_slot(variant);
+        if (na == 1 && masked && sv >= 0) {
           const StereoTgvImpl* s = act[0];
           if (level < (int)s->span_lo[sv].size()) {
             const std::vector<uint16_t>& lo = s->span_lo[sv][level];
@@ -553,7 +553,7 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
       // no pixel of column 0 is on
       s->tb_ok.assign(s->levels(), 1);
       s->tma_ok.assign(s->levels(), 1);
-      for (int v = 0; v < 3; v++) {
+      for (int v = 0; v < kIterSpanSlots; v++) {
         s->span_lo[v].assign(s->levels(), {});
         s->span_hi[v].assign(s->levels(), {});
       }
@@ -577,7 +577,9 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
               xmax[y] = std::max(xmax[y], x);
             }
         const int tiles_x = iter_tiles_x_of(w);
-        for (int v = 0; v < 3; v++) {
+        for (int v = 0; v < kIterVariants; v++) {
+          const int slot = iter_span_slot(v);
+          if (slot < 0 || !iter_variant_tiled(v)) continue;
           const int TH = kIterVariantRows[v];
           const int rows = (h + TH - 1) / TH;
           std::vector<uint16_t> lo(rows), hi(rows);
@@ -597,8 +599,8 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
             lo[r] = (uint16_t)(a / 31);
             hi[r] = (uint16_t)std::min(tiles_x - 1, b / 31 + (b % 31 == 30 ? 1 : 0));
           }
-          s->span_lo[v][l] = lo;
-          s->span_hi[v][l] = hi;
+          s->span_lo[slot][l] = lo;
+          s->span_hi[slot][l] = hi;
         }
       }
       s->codes_valid = true;

@@ -282,18 +282,26 @@ inline int tiles_of(int w, int h) { return tiles_x_of(w) * ((h + kFTH - 1) / kFT
 // Variant 18: k_fused_iter_tma (kernels_tma.cu), the 8-row tiles of variant 1 with every input
 // plane of the block's region brought into shared memory by bulk tensor copies (TMA); one pair
 // per launch, on levels where no pixel of column 0 is on (masked form).
+// Variant 19: k_fused_iter with 15-row tiles (512 threads, 4 blocks per SM): 64 resident
+// warps per SM, as against 63 with 8-row tiles, and 9 % of the threads on the halo, against
+// 14 %.
 // Numbers 3-5, 10-11 and 16-17 belonged to forms that never won on B200 (a warp streaming a
 // row strip, two pixels per thread, one cluster barrier per iteration) and were removed;
 // they are rejected, and the remaining numbers keep their meaning.
-constexpr int kIterVariants = 19;
-constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 0, 0, 0, 24, 24, 23, 17, 0, 0, 11, 5, 0, 0, 0, 0, 8};
-constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+constexpr int kIterVariants = 20;
+constexpr int kIterVariantRows[kIterVariants] = {4, 8, 16, 0, 0, 0, 24, 24, 23, 17, 0, 0, 11, 5, 0, 0, 0, 0, 8, 15};
+constexpr int kIterVariantMinBlocks[kIterVariants] = {12, 7, 3, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 4};
 constexpr int kIterTmaVariant = 18;
 constexpr int kIterFirstTBVariant = 6;
 inline bool iter_variant_retired(int v) { return (v >= 3 && v <= 5) || v == 10 || v == 11 || v == 16 || v == 17; }
 inline bool iter_variant_valid(int v) { return v >= 0 && v < kIterVariants && !iter_variant_retired(v); }
+// the k_fused_iter variants (one iteration per launch, one or several pairs per launch)
+inline bool iter_variant_tiled(int v) { return v == 0 || v == 1 || v == 2 || v == 19; }
+// per-row tile spans are kept for each k_fused_iter tile height; the slot of a variant
+constexpr int kIterSpanSlots = 4;
+inline int iter_span_slot(int v) { return v <= 2 ? v : v == 19 ? 3 : -1; }
 // variants whose launch carries one pair only (others fall back to the default there)
-inline bool iter_variant_single_pair(int v) { return v >= kIterFirstTBVariant; }
+inline bool iter_variant_single_pair(int v) { return v >= kIterFirstTBVariant && !iter_variant_tiled(v); }
 constexpr int kIterFirstDeepTBVariant = 12;
 constexpr int kIterFirstClusterVariant = 14;
 inline bool iter_variant_cluster(int v) { return v == kIterFirstClusterVariant || v == kIterFirstClusterVariant + 1; }

@@ -86,6 +86,42 @@ struct FusedIter {
     }
     return true;
   }
+
+  // dual_at for a pixel that is on and whose four neighbours are in the image (and, masked,
+  // on): the right and down neighbours are the ones used, and nothing depends on the code.
+  static __device__ __forceinline__ void dual_interior(const IterPair& P, const T2* pin, const T4* qin, int pos,
+                                                       float a, float b, float c, float sp, float sq, float& u_pos,
+                                                       float2& vp, float2& p, float4& q, float2& tp, bool want_th,
+                                                       float& u_th, float& Iu_th, float& Iz_th) {
+    const T2* v_ = (const T2*)P.v_;
+    u_pos = P.u_[pos];
+    vp = S::ld2(v_, pos);
+    float u_xn = P.u_[pos + 1];
+    float u_yn = P.u_[pos + P.s];
+    float2 v_xn = S::ld2(v_, pos + 1);
+    float2 v_yn = S::ld2(v_, pos + P.s);
+    p = S::ld2(pin, pos);
+    q = S::ld4(qin, pos);
+    if (want_th) {
+      u_th = P.u[pos];
+      Iu_th = P.Iu[pos];
+      Iz_th = P.Iz[pos];
+    }
+    if (kFast) {
+      fast::dual(true, true, u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
+      tp = fast::tp(a, b, c, p);
+    } else {
+      dual_math(true, true, u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
+      tp = tp_math(a, b, c, p);
+    }
+  }
+
+  // a pixel whose code (and, for the plain form, position) makes every edge rule of the
+  // threshold and primal steps take its interior branch
+  static __device__ __forceinline__ bool interior(uint8_t code, int ix, int iy, int w, int h) {
+    if (MASKED) return code == (kOn | kR | kL | kD | kU);
+    return (code & kOn) && ix >= 1 && iy >= 1 && ix + 1 < w && iy + 1 < h;
+  }
 };
 
 // The block is a 32 x (TH + 1) region: one image row segment per warp, the first
@@ -155,7 +191,18 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   // round before any issues the second, so it is skipped (a tile without a pixel on then
   // does its few loads and writes nothing, as before).
   if (MASKED && A.span_rows == 0 && !__syncthreads_or(in_img && (code & kOn))) return;
-  if (in_img) {
+  // A warp whose 32 pixels are all interior (on, with the four neighbours in the image and,
+  // masked, on) takes the same operations without any of the edge rules' selections; the
+  // fisheye mask's inside is most of the warps.
+  const bool inner = __all_sync(0xffffffffu, in_img && F::interior(code, ix, iy, P.w, P.h));
+  if (inner) {
+    F::dual_interior(P, pin, qin, pos, a, b, c, A.sp[pi_], A.sq[pi_], ubar, vb, pp, qq, tp, tile, u_th, Iu_th, Iz_th);
+    if (tile) {
+      S::st2(pout, pos, pp);
+      S::st4(qout, pos, qq);
+      if (A.write_tp) P.Tp[pos] = tp;
+    }
+  } else if (in_img) {
     bool own = F::dual_at(P, pin, qin, ix, iy, pos, code, a, b, c, A.sp[pi_], A.sq[pi_], ubar, vb, pp, qq, tp, tile,
                           u_th, Iu_th, Iz_th);
     if (own && tile) {
@@ -178,7 +225,12 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   // ---- phase 2: thresholding --------------------------------------------------------
   float dxm, dym;
   bool zR, zD, hasL, hasU;
-  if (MASKED) {
+  if (inner) {  // both neighbours of each difference exist: the central forms
+    dxm = tp.x - sTp[ry][rx - 1].x;
+    dym = tp.y - sTp[ry - 1][rx].y;
+    zR = zD = false;
+    hasL = hasU = true;
+  } else if (MASKED) {
     if (!(code & kOn)) return;
     bool mR = code & kR, mL = code & kL, mD = code & kD, mU = code & kU;
     if (mL && mR) dxm = tp.x - sTp[ry][rx - 1].x;
@@ -289,7 +341,7 @@ double iteration_gpu_share(int variant, bool masked, bool half, int w, int h) {
     return cluster_gpu_share(variant, w, h);
   } else if (variant == kIterTmaVariant) {
     return tma_gpu_share(masked, half, w, h);
-  } else if (variant >= kIterFirstTBVariant) {
+  } else if (variant >= kIterFirstTBVariant && !iter_variant_tiled(variant)) {
     return tb_gpu_share(variant, masked, half, w, h);
   } else {
     const int rows = kIterVariantRows[variant];
@@ -297,6 +349,7 @@ double iteration_gpu_share(int variant, bool masked, bool half, int w, int h) {
     switch (variant) {
       case 0: per_sm = blocks_per_sm_th<4, kIterVariantMinBlocks[0]>(masked, half); break;
       case 2: per_sm = blocks_per_sm_th<16, kIterVariantMinBlocks[2]>(masked, half); break;
+      case 19: per_sm = blocks_per_sm_th<15, kIterVariantMinBlocks[19]>(masked, half); break;
       default: per_sm = blocks_per_sm_th<8, kIterVariantMinBlocks[1]>(masked, half); break;
     }
   }
@@ -310,11 +363,14 @@ double iteration_gpu_share(int variant, bool masked, bool half, int w, int h) {
 void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, cudaStream_t st, int parity,
                             int variant) {
   if (A.ntiles <= 0) return;
-  static_assert(kIterVariantRows[0] == 4 && kIterVariantRows[1] == 8 && kIterVariantRows[2] == 16, "variants");
+  static_assert(kIterVariantRows[0] == 4 && kIterVariantRows[1] == 8 && kIterVariantRows[2] == 16 &&
+                    kIterVariantRows[19] == 15,
+                "variants");
   if (iter_variant_retired(variant) || variant == kIterTmaVariant) throw ArgError{"not a k_fused_iter variant"};
   switch (variant) {
     case 0: launch_iter_th<4, kIterVariantMinBlocks[0]>(A, masked, half_storage, st, parity); break;
     case 2: launch_iter_th<16, kIterVariantMinBlocks[2]>(A, masked, half_storage, st, parity); break;
+    case 19: launch_iter_th<15, kIterVariantMinBlocks[19]>(A, masked, half_storage, st, parity); break;
     default: launch_iter_th<8, kIterVariantMinBlocks[1]>(A, masked, half_storage, st, parity); break;
   }
   VFS_LAUNCH_CHECK();

@@ -180,7 +180,7 @@ class StereoTgvImpl {
   // per one-iteration tile variant (0-2) and level: for each tile row, the first and last
   // tile column whose region (tile + west / north halo) holds a pixel that is on (masked
   // form; first > last for a row without any)
-  std::vector<std::vector<uint16_t>> span_lo[3], span_hi[3];
+  std::vector<std::vector<uint16_t>> span_lo[kIterSpanSlots], span_hi[kIterSpanSlots];
   int f_parity = 0;      // which p / q plane holds the latest values
   int levels() const { return (int)pW.size(); }
   Geom geomAt(int level) const { return Geom{pW[level], pH[level], pS[level]}; }

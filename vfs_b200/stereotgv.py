@@ -121,7 +121,8 @@ class StereoTgv:
         check(self._h, self._L.vfs_set_autotune(self._h, int(on)))
 
     def set_iteration_variant(self, variant: int) -> None:
-        """Force one variant (0..17) of the fused iteration kernel, or -1 for the tuned choice."""
+        """Force one variant (0..19, the retired numbers excepted) of the fused iteration kernel,
+        or -1 for the tuned choice."""
         check(self._h, self._L.vfs_set_iteration_variant(self._h, int(variant)))
 
     def set_iteration_variants(self, variants) -> None:
@@ -333,7 +334,8 @@ class StereoBatch:
         check_batch(self._h, self._L.vfs_batch_set_autotune(self._h, int(on)))
 
     def set_iteration_variant(self, variant: int) -> None:
-        """Force one variant (0..17) of the fused iteration kernel, or -1 for the tuned choice."""
+        """Force one variant (0..19, the retired numbers excepted) of the fused iteration kernel,
+        or -1 for the tuned choice."""
         check_batch(self._h, self._L.vfs_batch_set_iteration_variant(self._h, int(variant)))
 
     def set_iteration_variants(self, variants) -> None:
