@@ -225,9 +225,14 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             if (!lo.empty() && (int)lo.size() <= kMaxSpanRows) {
               A.span_rows = (int)lo.size();
               A.span_max = 0;
+              const std::vector<uint16_t>& ilo = s->inner_lo[sv][level];
+              const std::vector<uint16_t>& ihi = s->inner_hi[sv][level];
+              const bool have_inner = ilo.size() == lo.size() && ihi.size() == lo.size();
               for (size_t r = 0; r < lo.size(); r++) {
                 A.span_lo[r] = lo[r];
                 A.span_hi[r] = hi[r];
+                A.in_lo[r] = have_inner ? ilo[r] : 1;
+                A.in_hi[r] = have_inner ? ihi[r] : 0;
                 if (hi[r] >= lo[r]) A.span_max = std::max(A.span_max, (int)hi[r] - (int)lo[r] + 1);
               }
             }
@@ -556,6 +561,8 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
       for (int v = 0; v < kIterSpanSlots; v++) {
         s->span_lo[v].assign(s->levels(), {});
         s->span_hi[v].assign(s->levels(), {});
+        s->inner_lo[v].assign(s->levels(), {});
+        s->inner_hi[v].assign(s->levels(), {});
       }
       for (int l = 0; l < s->levels(); l++) {
         const int w = s->pW[l], h = s->pH[l];
@@ -577,6 +584,13 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
               xmax[y] = std::max(xmax[y], x);
             }
         const int tiles_x = iter_tiles_x_of(w);
+        // per row, the number of pixels left of x that are not interior (edge code 0x1F: on,
+        // with the four neighbours in the image and on)
+        const uint8_t kInterior = kOn | kR | kL | kD | kU;
+        std::vector<int> notin((size_t)h * (w + 1), 0);
+        for (int y = 0; y < h; y++)
+          for (int x = 0; x < w; x++)
+            notin[(size_t)y * (w + 1) + x + 1] = notin[(size_t)y * (w + 1) + x] + (code[(size_t)y * w + x] != kInterior);
         for (int v = 0; v < kIterVariants; v++) {
           const int slot = iter_span_slot(v);
           if (slot < 0 || !iter_variant_tiled(v)) continue;
@@ -601,6 +615,34 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
           }
           s->span_lo[slot][l] = lo;
           s->span_hi[slot][l] = hi;
+          // the longest run of tiles whose region (rows TH r - 1 .. TH r + TH - 1, columns
+          // 31 tx - 1 .. 31 tx + 30) lies in the image and holds interior pixels only
+          std::vector<uint16_t> ilo(rows, 1), ihi(rows, 0);
+          for (int r = 0; r < rows; r++) {
+            const int y_lo = TH * r - 1, y_hi = TH * r + TH - 1;
+            if (y_lo < 0 || y_hi >= h) continue;
+            int run0 = -1, best_len = 0;
+            for (int tx = 0; tx <= tiles_x; tx++) {
+              bool ok = false;
+              const int x_lo = 31 * tx - 1, x_hi = 31 * tx + 30;
+              if (tx < tiles_x && x_lo >= 0 && x_hi < w) {
+                ok = true;
+                for (int y = y_lo; ok && y <= y_hi; y++)
+                  ok = notin[(size_t)y * (w + 1) + x_hi + 1] == notin[(size_t)y * (w + 1) + x_lo];
+              }
+              if (ok && run0 < 0) run0 = tx;
+              if (!ok && run0 >= 0) {
+                if (tx - run0 > best_len) {
+                  best_len = tx - run0;
+                  ilo[r] = (uint16_t)run0;
+                  ihi[r] = (uint16_t)(tx - 1);
+                }
+                run0 = -1;
+              }
+            }
+          }
+          s->inner_lo[slot][l] = ilo;
+          s->inner_hi[slot][l] = ihi;
         }
       }
       s->codes_valid = true;

@@ -115,6 +115,9 @@ struct IterArgs {
   // that is on); the others would write nothing.  span_max: the widest span (grid width).
   int span_rows, span_max;
   uint16_t span_lo[kMaxSpanRows], span_hi[kMaxSpanRows];
+  // With tile spans, tiles in_lo[r] .. in_hi[r] of tile row r (none where in_lo > in_hi) have
+  // a region whose every pixel is interior: on, with its four neighbours in the image and on.
+  uint16_t in_lo[kMaxSpanRows], in_hi[kMaxSpanRows];
 };
 // parity selects which half of the p / q ping-pong buffers is read (the other is written);
 // variant selects the tile height (kIterVariantRows[variant] rows of 31 pixels).

@@ -146,11 +146,13 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   const int pi_ = SINGLE ? 0 : find_pair(A.pr, A.npairs, t_);
   const IterPair& P = A.pr[pi_];
   int x0, y0;
+  bool blk_inner = false;  // every pixel of the block's region is interior (host-computed)
   if (SINGLE) {
     int tx = (int)blockIdx.x;
     if (MASKED && A.span_rows > 0) {  // only the tiles of this row that hold a pixel that is on
       tx += A.span_lo[blockIdx.y];
       if (tx > (int)A.span_hi[blockIdx.y]) return;
+      blk_inner = tx >= (int)A.in_lo[blockIdx.y] && tx <= (int)A.in_hi[blockIdx.y];
     }
     x0 = tx * 31;
     y0 = (int)blockIdx.y * TH;
@@ -179,7 +181,7 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   float a = 0.f, b = 0.f, c = 0.f, ubar = 0.f;
   float u_th = 0.f, Iu_th = 0.f, Iz_th = 0.f;
   if (in_img) {
-    code = P.code[pos];
+    if (!blk_inner) code = P.code[pos];
     a = P.a[pos];
     b = P.b[pos];
     c = P.c[pos];
@@ -193,8 +195,9 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   if (MASKED && A.span_rows == 0 && !__syncthreads_or(in_img && (code & kOn))) return;
   // A warp whose 32 pixels are all interior (on, with the four neighbours in the image and,
   // masked, on) takes the same operations without any of the edge rules' selections; the
-  // fisheye mask's inside is most of the warps.
-  const bool inner = __all_sync(0xffffffffu, in_img && F::interior(code, ix, iy, P.w, P.h));
+  // fisheye mask's inside is most of the warps.  In a block known to be interior nothing
+  // waits for the edge codes: its loads go out in one round.
+  const bool inner = blk_inner || __all_sync(0xffffffffu, in_img && F::interior(code, ix, iy, P.w, P.h));
   if (inner) {
     F::dual_interior(P, pin, qin, pos, a, b, c, A.sp[pi_], A.sq[pi_], ubar, vb, pp, qq, tp, tile, u_th, Iu_th, Iz_th);
     if (tile) {

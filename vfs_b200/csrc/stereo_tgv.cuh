@@ -181,6 +181,8 @@ class StereoTgvImpl {
   // tile column whose region (tile + west / north halo) holds a pixel that is on (masked
   // form; first > last for a row without any)
   std::vector<std::vector<uint16_t>> span_lo[kIterSpanSlots], span_hi[kIterSpanSlots];
+  // per tile row, the run of tiles whose region is all interior pixels (IterArgs::in_lo / in_hi)
+  std::vector<std::vector<uint16_t>> inner_lo[kIterSpanSlots], inner_hi[kIterSpanSlots];
   int f_parity = 0;      // which p / q plane holds the latest values
   int levels() const { return (int)pW.size(); }
   Geom geomAt(int level) const { return Geom{pW[level], pH[level], pS[level]}; }
