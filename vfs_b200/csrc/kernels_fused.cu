@@ -108,7 +108,7 @@ struct FusedIter {
       Iz_th = P.Iz[pos];
     }
     if (kFast) {
-      fast::dual(true, true, u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
+      fast::dual_interior(u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
       tp = fast::tp(a, b, c, p);
     } else {
       dual_math(true, true, u_pos, u_xn, u_yn, vp, v_xn, v_yn, a, b, c, sp, sq, p, q);
@@ -140,7 +140,9 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   typedef Store2<ST> S;
   constexpr bool kFast = F::kFast;
   __shared__ float2 sTp[TH + 1][32];
-  __shared__ float4 sQ[TH + 1][32];
+  // q of the region: the primal step reads (q.x, q.w) of the west and (q.z, q.y) of the north
+  // neighbour only
+  __shared__ float2 sQxw[TH + 1][32], sQzy[TH + 1][32];
   // one pair: a 2-D grid of tiles; several pairs: a 1-D grid over the pairs' tile ranges
   const int t_ = blockIdx.x;
   const int pi_ = SINGLE ? 0 : find_pair(A.pr, A.npairs, t_);
@@ -221,7 +223,8 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
     tp = P.Tp[pos];
   }
   sTp[ry][rx] = tp;
-  sQ[ry][rx] = qq;
+  sQxw[ry][rx] = make_float2(qq.x, qq.w);
+  sQzy[ry][rx] = make_float2(qq.z, qq.y);
   __syncthreads();
   if (!tile || !in_img) return;
 
@@ -278,14 +281,18 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   float4 qc = qq;
   if (zR) qc.x = qc.w = 0.0f;
   if (zD) qc.y = qc.z = 0.0f;
-  float4 ql = hasL ? sQ[ry][rx - 1] : make_float4(0.f, 0.f, 0.f, 0.f);
-  float4 qu = hasU ? sQ[ry - 1][rx] : make_float4(0.f, 0.f, 0.f, 0.f);
+  const float2 qxw_l = hasL ? sQxw[ry][rx - 1] : make_float2(0.f, 0.f);
+  const float2 qzy_u = hasU ? sQzy[ry - 1][rx] : make_float2(0.f, 0.f);
+  const float4 ql = make_float4(qxw_l.x, 0.f, 0.f, qxw_l.y), qu = make_float4(0.f, qzy_u.y, qzy_u.x, 0.f);
   float us_;
   float2 vs;
   if (kFast) {
     const float a1s = P.alpha1 * P.alpha1, a0s4 = 4.0f * P.alpha0 * P.alpha0;
     float ev1 = fast::etav(b, c, a1s, a0s4), ev2 = fast::etav(a, c, a1s, a0s4);
-    fast::primal(qc, ql, qu, tp, ev1, ev2, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs);
+    if (inner)
+      fast::primal_interior(qq, qxw_l, qzy_u, tp, ev1, ev2, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs);
+    else
+      fast::primal(qc, ql, qu, tp, ev1, ev2, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs);
   } else {
     float ev1 = etav1_math(b, c, P.alpha0, P.alpha1), ev2 = etav2_math(a, c, P.alpha0, P.alpha1);
     float2 vo;

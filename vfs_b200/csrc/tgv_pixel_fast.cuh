@@ -26,6 +26,43 @@ __device__ __forceinline__ float rsqrt(float x) {
   return r;
 }
 
+// Pairs of floats on the packed FP32 instructions of sm_100 (add / sub / mul / fma .rn.f32x2,
+// no flush to zero): each lane is the IEEE single-precision operation of the scalar form, so
+// a packed step gives the bits of the two scalar steps it replaces.
+namespace x2 {
+typedef unsigned long long f2;
+__device__ __forceinline__ f2 pk(float x, float y) {
+  f2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(x), "f"(y));
+  return r;
+}
+__device__ __forceinline__ float2 upk(f2 r) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(r));
+  return v;
+}
+__device__ __forceinline__ f2 add(f2 a, f2 b) {
+  f2 d;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 sub(f2 a, f2 b) {
+  f2 d;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 mul(f2 a, f2 b) {
+  f2 d;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+  return d;
+}
+__device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) {
+  f2 d;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+  return d;
+}
+}  // namespace x2
+
 // Dual update.  A forward difference (right / down neighbour) and a backward one (left /
 // up) differ only in sign, so each is written as sgn * (neighbour - centre); the sign
 // change is exact.  The projection onto the unit ball multiplies by 1 / |p| where |p| > 1
@@ -53,6 +90,40 @@ __device__ __forceinline__ void dual(bool useRight, bool useDown, float u_pos, f
   float qy = __fmaf_rn(qsy, v_yn.y - vp.y, q.y);
   float qz = __fmaf_rn(qsy, v_yn.x - vp.x, q.z);
   float qw = __fmaf_rn(qsx, v_xn.y - vp.y, q.w);
+  float m2 = __fmaf_rn(qx, qx, __fmaf_rn(qy, qy, __fmaf_rn(qz, qz, qw * qw)));
+  if (!(m2 <= 1.0f)) {
+    float r = rsqrt(m2);
+    qx *= r;
+    qy *= r;
+    qz *= r;
+    qw *= r;
+  }
+  q = make_float4(qx, qy, qz, qw);
+}
+
+// dual() at a pixel whose right and down neighbours are the ones used (sx = sy = 1), with the
+// x / y and q lanes paired.  fma(1, d, -v) and d - v round the same exact value once, and
+// sq * 1 is exact, so every lane is the scalar form's operation.
+__device__ __forceinline__ void dual_interior(float u_pos, float u_xn, float u_yn, float2 vp, float2 v_xn,
+                                              float2 v_yn, float a, float b, float c, float sp, float sq, float2& p,
+                                              float4& q) {
+  using namespace x2;
+  const f2 vpp = pk(vp.x, vp.y);
+  const float2 u = upk(sub(sub(pk(u_xn, u_yn), pk(u_pos, u_pos)), vpp));
+  float dtx = __fmaf_rn(a, u.x, c * u.y);
+  float dty = __fmaf_rn(c, u.x, b * u.y);
+  float2 pp = upk(fma(pk(sp, sp), pk(dtx, dty), pk(p.x, p.y)));
+  float n2 = __fmaf_rn(pp.x, pp.x, pp.y * pp.y);
+  if (!(n2 <= 1.0f)) {
+    float r = rsqrt(n2);
+    pp.x *= r;
+    pp.y *= r;
+  }
+  p = pp;
+  const f2 s2 = pk(sq, sq);
+  const float2 qxw = upk(fma(s2, sub(pk(v_xn.x, v_xn.y), vpp), pk(q.x, q.w)));
+  const float2 qzy = upk(fma(s2, sub(pk(v_yn.x, v_yn.y), vpp), pk(q.z, q.y)));
+  float qx = qxw.x, qw = qxw.y, qz = qzy.x, qy = qzy.y;
   float m2 = __fmaf_rn(qx, qx, __fmaf_rn(qy, qy, __fmaf_rn(qz, qz, qw * qw)));
   if (!(m2 <= 1.0f)) {
     float r = rsqrt(m2);
@@ -119,6 +190,25 @@ __device__ __forceinline__ void primal(float4 qc, float4 ql, float4 qu, float2 t
   }
   u_s = __fmaf_rn(mu, u_new - u_bar, u_new);
   v_s = make_float2(__fmaf_rn(mu, vx - vb.x, vx), __fmaf_rn(mu, vy - vb.y, vy));
+}
+
+// primal() with the x / y lanes paired (the same operations lane by lane).  qxw_l = (q.x, q.w)
+// of the west neighbour, qzy_u = (q.z, q.y) of the north one.
+__device__ __forceinline__ void primal_interior(float4 qc, float2 qxw_l, float2 qzy_u, float2 tpp, float ev1,
+                                                float ev2, float tau, float alpha0, float alpha1, float mu, float2 vb,
+                                                float u_new, float u_bar, float& u_s, float2& v_s) {
+  using namespace x2;
+  const f2 dq = add(sub(pk(qc.x, qc.w), pk(qxw_l.x, qxw_l.y)), sub(pk(qc.z, qc.y), pk(qzy_u.x, qzy_u.y)));
+  const f2 g = fma(pk(alpha1, alpha1), pk(tpp.x, tpp.y), mul(pk(alpha0, alpha0), dq));
+  const f2 vbb = pk(vb.x, vb.y);
+  f2 v;
+  if (ev2 != 0.0f) {
+    v = fma(pk(ev1 != 0.0f ? tau * rcp(ev1) : tau, tau * rcp(ev2)), g, vbb);
+  } else {  // updatePrimalVariables.cu:103-105 writes .x again; .y keeps the previous value
+    v = pk(__fmaf_rn(tau, upk(g).x, vb.x), vb.y);
+  }
+  u_s = __fmaf_rn(mu, u_new - u_bar, u_new);
+  v_s = upk(fma(pk(mu, mu), sub(v, vbb), v));
 }
 
 }  // namespace fast
