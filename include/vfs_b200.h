@@ -77,6 +77,12 @@ int vfs_set_warm_start(vfs_stereo* s, int level);
  * reference).  Graphs captured for an older mask or initialize are destroyed on the next
  * solve, and at most 64 are kept (vfs_batch_cached_graphs: the same for a batch). */
 int vfs_cached_graphs(const vfs_stereo* s);
+/* Number of fused solves this process has run while timing the iteration-kernel variants (the
+ * first solve of a new setting; no counterpart in the reference).  A one-pair solve reuses
+ * every pyramid level tuned before for the same level size, form and storage (the choice made
+ * for a pair alone or with other pairs in flight, the same setting first), so a server whose
+ * batch compositions change tunes only for level sizes it has not seen. */
+long long vfs_tuning_solves(void);
 
 /* Whole-state export / import (no counterpart in the reference): the handle's device state
  * (image pyramid, mask, fields, every solver buffer with the stale values the reference keeps

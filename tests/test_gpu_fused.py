@@ -269,6 +269,45 @@ def test_per_level_variants_and_tuned_choice_reported(gpu):
     assert len(v) == 3 and all(x in VARIANTS for x in v)
 
 
+def test_new_batch_compositions_reuse_tuned_levels(gpu):
+    """Each pair of a concurrent batch is tuned per pyramid level: a batch of a new composition
+    (here two of the three pairs) reuses the levels tuned with other pairs in flight, and so does
+    a pair solved alone once its level sizes were tuned in a batch; no tuning solve runs again.
+    Results are the drop-in path's."""
+    from vfs_b200._native import lib
+    from vfs_b200.stereotgv import StereoBatch
+    count = lambda: lib().vfs_tuning_solves()
+    p = params(n_levels=3, n_warp=2, n_iter=9)
+    cases = [random_case(152, 136, seed=4100 + k) for k in range(4)]
+    pairs = [make(*c, p, fused=True) for c in cases]
+    for s in pairs:
+        s.set_autotune(True)
+
+    def batch_solve(members):
+        b = StereoBatch(half_storage=False)
+        for m in members:
+            b.add(m)
+        for m, c in zip(members, cases):
+            m.copyImagesToDevice(c[0], c[1])
+        b.solve(True)
+        for m in members:
+            m.synchronize()
+
+    batch_solve(pairs[:3])  # tunes (unless an earlier test tuned these level sizes)
+    n0 = count()
+    batch_solve(pairs[:2])  # a new composition, pairs still in flight together
+    batch_solve([pairs[0], pairs[3]])
+    assert count() == n0
+    solve_frames(pairs[1], cases[1][0], cases[1][1], True, 1)  # alone
+    solve_frames(pairs[2], cases[2][0], cases[2][1], True, 2)
+    assert count() == n0
+    ref = make(*cases[2], p, fused=False)
+    solve_frames(ref, cases[2][0], cases[2][1], True, 1)
+    one = make(*cases[2], p, fused=True)
+    solve_frames(one, cases[2][0], cases[2][1], True, 1)
+    assert np.array_equal(one.debug_buffer("u", 1), ref.debug_buffer("u", 1))
+
+
 def test_retired_variants_are_rejected(gpu):
     """Numbers of the removed forms (3-5, 10-11, 16-17) and out-of-range numbers are refused."""
     from vfs_b200.stereotgv import VfsError

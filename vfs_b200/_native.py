@@ -48,6 +48,7 @@ SIGNATURES = {
     "vfs_set_warm_start": [_vp, _i],
     "vfs_cached_graphs": [_vp],
     "vfs_batch_cached_graphs": [_vp],
+    "vfs_tuning_solves": [],
     "vfs_state_bytes": [_vp],
     "vfs_export_state": [_vp, _vp, _sz],
     "vfs_import_state": [_vp, _vp, _sz],
@@ -113,6 +114,7 @@ SIGNATURES = {
 _RESTYPE = {
     "vfs_estimate_device_bytes": ctypes.c_size_t,
     "vfs_launch_count": ctypes.c_longlong,
+    "vfs_tuning_solves": ctypes.c_longlong,
     "vfs_state_bytes": ctypes.c_size_t,
     "vfs_status_string": ctypes.c_char_p,
     "vfs_last_error": ctypes.c_char_p,

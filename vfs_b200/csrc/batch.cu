@@ -5,6 +5,7 @@
 // its own coarsest level.
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -305,10 +306,22 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             if (!iter_variant_valid(v)) continue;
             const int kv = tb_iterations(v);
             if (kv > 1 && (!tb_here || kv > P0.nSolverIters)) continue;
+            // Several iterations per launch recompute the tile halos, which pays only for a pair
+            // alone: in the 8-pair 848x800 batch they cost 6-12 % of the step at 212 x 200.
+            if (kv > 1 && concurrency > 1) continue;
             if (iter_variant_single_pair(v) && na != 1) continue;
-            if (v == kIterTmaVariant && !tma_here) continue;
+            // The TMA-staged kernel has no interior-warp path and is slower than variant 1;
+            // per-launch timings amid other pairs' work still picked it at 424 x 400, where it
+            // cost 2 % of the 8-pair step.  It runs when forced.
+            if (v == kIterTmaVariant) continue;
             const bool clv = iter_variant_cluster(v);
             if (clv && (!tb_here || !cluster_fits(v, masked, half, lw, lh))) continue;
+            // With other pairs in flight, a cluster whose threads each hold several pixels takes
+            // that many times longer per iteration while it holds a whole cluster of SMs: on
+            // B200 the 8-pair 848x800 batch ran 4.5 % slower with it at 212 x 200 (3 pixels per
+            // thread) than with one-iteration launches there, which per-launch timings taken
+            // amid the other pairs' work did not show.  It stays a candidate for a pair alone.
+            if (clv && concurrency > 1 && cluster_pixels_per_thread(v, half, lw, lh) > 1) continue;
             // the cluster-resident kernel is timed over an odd number of iterations, so that it
             // writes the other ping-pong buffers, which the first iteration below overwrites
             const int kc = clv ? ((std::min(P0.nSolverIters, kCLMaxIters) - 1) | 1) : 1;
@@ -491,6 +504,20 @@ std::map<std::vector<int>, std::vector<int>>& shared_tuned() {
   static std::map<std::vector<int>, std::vector<int>> m;
   return m;
 }
+// Tuned choices of one-pair solves per level: form, storage, alone or with other pairs in
+// flight, and the level's width and height.  A one-pair engine (each pair of a concurrent
+// batch, each request of the server) takes a level's choice from here when that level was
+// tuned before in the same setting, whatever the rest of the batch, so a new batch
+// composition does not stop the stream to time every variant again.
+std::map<std::array<int, 5>, int>& shared_level_tuned() {
+  static std::map<std::array<int, 5>, int> m;
+  return m;
+}
+std::atomic<long long>& tuning_solves() {
+  static std::atomic<long long> n{0};
+  return n;
+}
+long long tuning_solve_count() { return tuning_solves().load(std::memory_order_relaxed); }
 std::mutex& shared_tuned_mutex() {
   static std::mutex m;
   return m;
@@ -681,20 +708,44 @@ void FusedEngine::solve_parts(std::vector<StereoTgvImpl*>& pairs, bool masked, b
   for (auto* s : pairs) max_top = std::max(max_top, s->topLevel());
   auto in_part = [&](int l) { return !((part == 1 && l == 0) || (part == 2 && l > 0)) && l <= max_top; };
   bool need_tune = false;
+  const bool one_pair = pairs.size() == 1;
+  auto level_key = [&](int l) {
+    return std::array<int, 5>{(int)masked, (int)half, concurrency > 1 ? 2 : 1, pairs[0]->pW[l], pairs[0]->pH[l]};
+  };
   if (autotune && !forced) {
     // a composition tuned before (by any engine of the process) is reused, so that every
-    // pair of a batch runs the same choice and only the first tunes
+    // pair of a batch runs the same choice and only the first tunes; a one-pair solve also
+    // reuses any level tuned before in the same setting
     std::lock_guard<std::mutex> lk(shared_tuned_mutex());
     auto& shared = shared_tuned();
     auto sit = shared.find(comp);
     for (int l = 0; l < maxL; l++) {
       if (!in_part(l) || tit->second[l] >= 0) continue;
-      if (sit != shared.end() && l < (int)sit->second.size() && sit->second[l] >= 0) tit->second[l] = sit->second[l];
-      else need_tune = true;
+      if (sit != shared.end() && l < (int)sit->second.size() && sit->second[l] >= 0) {
+        tit->second[l] = sit->second[l];
+        continue;
+      }
+      if (one_pair && l < pairs[0]->levels()) {
+        // the same setting first; else the choice made for this level size in the other
+        // setting (alone / with other pairs in flight), so that a level size is timed once
+        // and a server never stops a stream for a setting it has not met before
+        auto key = level_key(l);
+        auto lit = shared_level_tuned().find(key);
+        if (lit == shared_level_tuned().end()) {
+          key[2] = key[2] == 1 ? 2 : 1;
+          lit = shared_level_tuned().find(key);
+        }
+        if (lit != shared_level_tuned().end()) {
+          tit->second[l] = lit->second;
+          continue;
+        }
+      }
+      need_tune = true;
     }
   }
   if (need_tune) {
     // first solve of this composition (and part): run it directly and tune while it runs
+    tuning_solves().fetch_add(1, std::memory_order_relaxed);
     std::vector<int> lv = tit->second;
     fused_solve_direct(pairs, masked, half, st, lv, true, concurrency, part);
     tit->second = lv;
@@ -703,7 +754,10 @@ void FusedEngine::solve_parts(std::vector<StereoTgvImpl*>& pairs, bool masked, b
       std::vector<int>& sv = shared_tuned()[comp];
       sv.resize(maxL, -1);
       for (int l = 0; l < maxL; l++)
-        if (in_part(l) && lv[l] >= 0) sv[l] = lv[l];
+        if (in_part(l) && lv[l] >= 0) {
+          sv[l] = lv[l];
+          if (one_pair && l < pairs[0]->levels()) shared_level_tuned().emplace(level_key(l), lv[l]);
+        }
     }
     note_variants(lv, part);
     return;

@@ -172,6 +172,7 @@ int vfs_set_limit_range(vfs_stereo* s, float lr) {
 
 int vfs_cached_graphs(const vfs_stereo* s) { return s ? (int)s->impl.engine.graphs() : VFS_ERR_ARG; }
 int vfs_batch_cached_graphs(const vfs_batch* b) { return b ? (int)b->engine.graphs() : VFS_ERR_ARG; }
+long long vfs_tuning_solves(void) { return vfs::tuning_solve_count(); }
 
 int vfs_set_warm_start(vfs_stereo* s, int level) {
   return guarded(s, [&] {

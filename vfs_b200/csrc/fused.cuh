@@ -153,6 +153,10 @@ int cluster_ctas(int variant);
 int cluster_rows(int variant, int h);
 // the level's state fits the cluster's shared memory and such a cluster can be resident
 bool cluster_fits(int variant, bool masked, bool half, int w, int h);
+// solves of the process that timed iteration-kernel variants (vfs_tuning_solves)
+long long tuning_solve_count();
+// owned pixels per thread of the cluster-resident kernel on a w x h level (0: not a cluster variant)
+int cluster_pixels_per_thread(int variant, bool half, int w, int h);
 double cluster_gpu_share(int variant, int w, int h);
 void launch_fused_iteration_cluster(const IterCLArgs& A, bool masked, bool half_storage, cudaStream_t st,
                                     int variant);

@@ -401,6 +401,11 @@ bool cluster_fits(int variant, bool masked, bool half, int w, int h) {
   return ok;
 }
 
+int cluster_pixels_per_thread(int variant, bool half, int w, int h) {
+  if (cluster_ctas(variant) <= 0 || w <= 0 || h <= 0) return 0;
+  return geometry_of(variant, half, w, h).ppt;
+}
+
 int cluster_rows(int variant, int h) {
   const int ctas = cluster_ctas(variant);
   return ctas > 0 ? (h + ctas - 1) / ctas : 0;
