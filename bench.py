@@ -733,9 +733,9 @@ def run_serving(args, emit=True):
         srv = StereoServer(reserve_bytes=1 << 30, **kw)
         for sid, (w, h, fields, frames) in data.items():
             srv.open_stream(sid, w, h, fields["mask"], fields["tv"], fields["cv"], synth.n_levels_for(w), params)
-        # warm the server with two frames per stream (each pair's graphs are captured for
-        # both of its pointer states)
-        for _ in range(2):
+        # warm the server with four frames per stream, so that each pair's graphs are captured
+        # for the buffer assignments its frames cycle through before the timed replay
+        for _ in range(4):
             for sid, (w, h, fields, frames) in data.items():
                 srv.submit(sid, *frames[0])
             srv.run_until_idle()

@@ -130,11 +130,25 @@ class StereoServer:
         self.done: List[Request] = []
         self._seq = 0
         self.counters = collections.Counter()  # deferred admissions, parks, unparks, cancels
+        self._free_val: Optional[int] = None
+        self._free_t = 0.0
 
     # ---- memory -----------------------------------------------------------------------
-    def _free(self) -> int:
-        free, _ = self.torch.cuda.mem_get_info(self.device)
-        return int(free)
+    # A free-memory reading is reused for up to this long unless the server itself allocates or
+    # releases a stream's state in between (which forgets it).  The driver query takes up to
+    # tens of milliseconds while the GPU is busy, and the admission pass would otherwise make
+    # one per waiting request on every scheduling pass.
+    FREE_TTL_S = 1.0
+
+    def _free(self, fresh: bool = False) -> int:
+        now = time.perf_counter()
+        if fresh or self._free_val is None or now - self._free_t > self.FREE_TTL_S:
+            free, _ = self.torch.cuda.mem_get_info(self.device)
+            self._free_val, self._free_t = int(free), now
+        return self._free_val
+
+    def _forget_free(self) -> None:
+        self._free_val = None
 
     def _state_bytes(self, cam: _Camera, fused: bool) -> int:
         return int(lib().vfs_estimate_device_bytes(cam.width, cam.height, cam.n_levels, cam.params["fScale"], 32,
@@ -176,6 +190,7 @@ class StereoServer:
         self.cameras[stream_id] = cam
 
     def _new_solver(self, cam: _Camera) -> StereoTgv:
+        self._forget_free()
         p = cam.params
         s = StereoTgv()
         s.set_solve_path(self.path != "plain", self.half)
@@ -192,6 +207,7 @@ class StereoServer:
                 lane.batch.clear()
         cam.solver.close()
         cam.solver = None
+        self._forget_free()
 
     def park_stream(self, stream_id: int) -> None:
         """Move an idle stream's state to page-locked host memory and free its device memory."""
@@ -225,8 +241,10 @@ class StereoServer:
         until `need` bytes fit beside the reserve."""
         if need + self.reserve <= self._free():
             return True
+        if need + self.reserve <= self._free(fresh=True):
+            return True
         self.torch.cuda.empty_cache()  # memory torch keeps cached is not free to the driver
-        if need + self.reserve <= self._free():
+        if need + self.reserve <= self._free(fresh=True):
             return True
         waiting = {r.stream_id for r in self.queue}
         idle = [c for c in self.cameras.values()
@@ -235,9 +253,9 @@ class StereoServer:
         for c in idle:
             self.park_stream(c.stream_id)
             self.torch.cuda.synchronize(self.device)
-            if need + self.reserve <= self._free():
+            if need + self.reserve <= self._free(fresh=True):
                 return True
-        return need + self.reserve <= self._free()
+        return need + self.reserve <= self._free(fresh=True)
 
     def close_stream(self, stream_id: int) -> None:
         """Close a stream between its frames; its waiting requests are cancelled."""
@@ -367,7 +385,10 @@ class StereoServer:
             ev = torch.cuda.Event()
             ev.record(st)
         for r in picked:
-            self.cameras[r.stream_id].fused_ready = self.path != "plain"
+            cam = self.cameras[r.stream_id]
+            if not cam.fused_ready and self.path != "plain":
+                self._forget_free()  # the first fused solve allocates the fused state
+            cam.fused_ready = self.path != "plain"
         lane.ins, lane.outs, lane.hosts = ins, outs, hosts  # kept alive until the batch completes
         lane.event = ev
         lane.requests = picked
