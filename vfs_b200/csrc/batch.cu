@@ -309,6 +309,11 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
             // Several iterations per launch recompute the tile halos, which pays only for a pair
             // alone: in the 8-pair 848x800 batch they cost 6-12 % of the step at 212 x 200.
             if (kv > 1 && concurrency > 1) continue;
+            // Nor do the other tile heights of the one-iteration kernel: in the 8-pair batch none
+            // beat variant 1 by more than the run-to-run spread at any level (15 rows: 0-2 %
+            // slower at 848 x 800; 16 rows: 5 % slower; 4 rows: equal at 212 x 200), while the
+            // tuner's timings amid the other pairs' work picked them by mistake (a 2 % loss).
+            if (concurrency > 1 && iter_variant_tiled(v) && v != kIterDefaultVariant) continue;
             if (iter_variant_single_pair(v) && na != 1) continue;
             // The TMA-staged kernel has no interior-warp path and is slower than variant 1;
             // per-launch timings amid other pairs' work still picked it at 424 x 400, where it
