@@ -76,8 +76,9 @@ __device__ __forceinline__ void dual(bool useRight, bool useDown, float u_pos, f
   float u_y = __fmaf_rn(sy, u_yn - u_pos, -vp.y);
   float dtx = __fmaf_rn(a, u_x, c * u_y);
   float dty = __fmaf_rn(c, u_x, b * u_y);
-  float ppx = __fmaf_rn(sp, dtx, p.x);
-  float ppy = __fmaf_rn(sp, dty, p.y);
+  // p and the q lanes (x, w) / (z, y) in pairs on the packed instructions (namespace x2)
+  float2 pp = x2::upk(x2::fma(x2::pk(sp, sp), x2::pk(dtx, dty), x2::pk(p.x, p.y)));
+  float ppx = pp.x, ppy = pp.y;
   float n2 = __fmaf_rn(ppx, ppx, ppy * ppy);
   if (!(n2 <= 1.0f)) {
     float r = rsqrt(n2);
@@ -86,10 +87,10 @@ __device__ __forceinline__ void dual(bool useRight, bool useDown, float u_pos, f
   }
   p = make_float2(ppx, ppy);
   const float qsx = sq * sx, qsy = sq * sy;  // exact: a sign change
-  float qx = __fmaf_rn(qsx, v_xn.x - vp.x, q.x);
-  float qy = __fmaf_rn(qsy, v_yn.y - vp.y, q.y);
-  float qz = __fmaf_rn(qsy, v_yn.x - vp.x, q.z);
-  float qw = __fmaf_rn(qsx, v_xn.y - vp.y, q.w);
+  const x2::f2 vpp = x2::pk(vp.x, vp.y);
+  const float2 qxw = x2::upk(x2::fma(x2::pk(qsx, qsx), x2::sub(x2::pk(v_xn.x, v_xn.y), vpp), x2::pk(q.x, q.w)));
+  const float2 qzy = x2::upk(x2::fma(x2::pk(qsy, qsy), x2::sub(x2::pk(v_yn.x, v_yn.y), vpp), x2::pk(q.z, q.y)));
+  float qx = qxw.x, qw = qxw.y, qz = qzy.x, qy = qzy.y;
   float m2 = __fmaf_rn(qx, qx, __fmaf_rn(qy, qy, __fmaf_rn(qz, qz, qw * qw)));
   if (!(m2 <= 1.0f)) {
     float r = rsqrt(m2);
@@ -172,28 +173,11 @@ __device__ __forceinline__ float threshold(float dxm, float dym, float eu, float
   return upos + d;
 }
 
-// Primal update of v and the over-relaxation of u and v; tpp = T p at this pixel.
-__device__ __forceinline__ void primal(float4 qc, float4 ql, float4 qu, float2 tpp, float ev1, float ev2, float tau,
-                                       float alpha0, float alpha1, float mu, float2 vb, float u_new, float u_bar,
-                                       float& u_s, float2& v_s) {
-  float dqx = (qc.x - ql.x) + (qc.z - qu.z);
-  float dqy = (qc.w - ql.w) + (qc.y - qu.y);
-  float gx = __fmaf_rn(alpha1, tpp.x, alpha0 * dqx);
-  float gy = __fmaf_rn(alpha1, tpp.y, alpha0 * dqy);
-  float vx, vy;
-  if (ev2 != 0.0f) {
-    vx = __fmaf_rn(ev1 != 0.0f ? tau * rcp(ev1) : tau, gx, vb.x);
-    vy = __fmaf_rn(tau * rcp(ev2), gy, vb.y);
-  } else {  // updatePrimalVariables.cu:103-105 writes .x again; .y keeps the previous value
-    vx = __fmaf_rn(tau, gx, vb.x);
-    vy = vb.y;
-  }
-  u_s = __fmaf_rn(mu, u_new - u_bar, u_new);
-  v_s = make_float2(__fmaf_rn(mu, vx - vb.x, vx), __fmaf_rn(mu, vy - vb.y, vy));
-}
-
-// primal() with the x / y lanes paired (the same operations lane by lane).  qxw_l = (q.x, q.w)
-// of the west neighbour, qzy_u = (q.z, q.y) of the north one.
+// Primal update with the x / y lanes paired: dq = (q.x - ql.x) + (q.z - qu.z) and
+// (q.w - ql.w) + (q.y - qu.y), g = alpha1 T p + alpha0 dq, v = v-bar + (tau / eta_v) g (the
+// eta_v2 = 0 case of updatePrimalVariables.cu:103-105 writes .x again and keeps .y), then the
+// over-relaxation.  qxw_l = (q.x, q.w) of the west neighbour, qzy_u = (q.z, q.y) of the north
+// one (zero where absent).
 __device__ __forceinline__ void primal_interior(float4 qc, float2 qxw_l, float2 qzy_u, float2 tpp, float ev1,
                                                 float ev2, float tau, float alpha0, float alpha1, float mu, float2 vb,
                                                 float u_new, float u_bar, float& u_s, float2& v_s) {
@@ -209,6 +193,16 @@ __device__ __forceinline__ void primal_interior(float4 qc, float2 qxw_l, float2 
   }
   u_s = __fmaf_rn(mu, u_new - u_bar, u_new);
   v_s = upk(fma(pk(mu, mu), sub(v, vbb), v));
+}
+
+
+// Primal update of v and the over-relaxation of u and v; tpp = T p at this pixel; ql / qu: q
+// of the west / north neighbour (zero where absent), of which the step reads (x, w) / (z, y).
+__device__ __forceinline__ void primal(float4 qc, float4 ql, float4 qu, float2 tpp, float ev1, float ev2, float tau,
+                                       float alpha0, float alpha1, float mu, float2 vb, float u_new, float u_bar,
+                                       float& u_s, float2& v_s) {
+  primal_interior(qc, make_float2(ql.x, ql.w), make_float2(qu.z, qu.y), tpp, ev1, ev2, tau, alpha0, alpha1, mu, vb,
+                  u_new, u_bar, u_s, v_s);
 }
 
 }  // namespace fast

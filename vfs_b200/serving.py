@@ -88,7 +88,8 @@ class _Lane:
     ins: list = field(default_factory=list)
     outs: list = field(default_factory=list)
     hosts: list = field(default_factory=list)
-    # page-locked staging reused from batch to batch: shape -> list of (i0, i1, u) host tensors
+    # buffers reused from batch to batch: shape -> list of page-locked (i0, i1, u) host tensors
+    # followed by their device counterparts
     pinned: Dict[tuple, list] = field(default_factory=dict)
 
     @property
@@ -131,21 +132,22 @@ class StereoServer:
         self._seq = 0
         self.counters = collections.Counter()  # deferred admissions, parks, unparks, cancels
         self._free_val: Optional[int] = None
-        self._free_t = 0.0
+        self._free_reserved = 0
 
     # ---- memory -----------------------------------------------------------------------
-    # A free-memory reading is reused for up to this long unless the server itself allocates or
-    # releases a stream's state in between (which forgets it).  The driver query takes up to
-    # tens of milliseconds while the GPU is busy, and the admission pass would otherwise make
-    # one per waiting request on every scheduling pass.
-    FREE_TTL_S = 1.0
-
     def _free(self, fresh: bool = False) -> int:
-        now = time.perf_counter()
-        if fresh or self._free_val is None or now - self._free_t > self.FREE_TTL_S:
-            free, _ = self.torch.cuda.mem_get_info(self.device)
-            self._free_val, self._free_t = int(free), now
-        return self._free_val
+        """Free device memory.  The driver's figure (cudaMemGetInfo) took up to 195 ms per query
+        while the GPU was busy, so it is read only when the server's own allocations or releases
+        of stream state have made the last reading stale, when a request does not fit by the
+        last reading, or when `fresh`; in between, memory the framework's caching allocator has
+        reserved since the reading is taken off it.  Memory that another process takes in
+        between is seen at the next reading."""
+        torch = self.torch
+        reserved = int(torch.cuda.memory_reserved(self.device))
+        if fresh or self._free_val is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            self._free_val, self._free_reserved = int(free), reserved
+        return self._free_val - max(0, reserved - self._free_reserved)
 
     def _forget_free(self) -> None:
         self._free_val = None
@@ -188,6 +190,12 @@ class StereoServer:
         cam.solver.loadVectorFields(cam.tv, cam.cv)
         cam.last_used = time.perf_counter()
         self.cameras[stream_id] = cam
+        # staging (page-locked and device) for as many frames of this size as a batch can hold:
+        # allocating it inside the serving loop stalled the loop for up to 113 ms while the GPU
+        # was busy
+        n = sum(1 for c in self.cameras.values() if (c.height, c.width) == (height, width))
+        for lane in self.lanes:
+            self._staging(lane, height, width, min(n, self.max_batch) - 1)
 
     def _new_solver(self, cam: _Camera) -> StereoTgv:
         self._forget_free()
@@ -337,13 +345,19 @@ class StereoServer:
         return picked
 
     def _staging(self, lane: _Lane, h: int, w: int, k: int):
-        """The k-th page-locked (i0, i1, u) staging set of a lane for h x w frames."""
+        """The k-th buffer set of a lane for h x w frames: page-locked (i0, i1, u) and the
+        device (i0, i1, u) the batch reads and writes.  A lane reuses them only once its
+        previous batch has completed."""
         pool = lane.pinned.setdefault((h, w), [])
         torch = self.torch
         while len(pool) <= k:
-            pool.append((torch.empty((h, w), dtype=torch.uint8).pin_memory(),
-                         torch.empty((h, w), dtype=torch.uint8).pin_memory(),
-                         torch.empty((h, w), dtype=torch.float32).pin_memory()))
+            with torch.cuda.stream(lane.stream):  # device blocks of the lane's stream
+                pool.append((torch.empty((h, w), dtype=torch.uint8).pin_memory(),
+                             torch.empty((h, w), dtype=torch.uint8).pin_memory(),
+                             torch.empty((h, w), dtype=torch.float32).pin_memory(),
+                             torch.empty((h, w), dtype=torch.uint8, device=self.device),
+                             torch.empty((h, w), dtype=torch.uint8, device=self.device),
+                             torch.empty((h, w), dtype=torch.float32, device=self.device)))
         return pool[k]
 
     def _launch(self, lane: _Lane) -> bool:
@@ -362,12 +376,14 @@ class StereoServer:
                 cam.busy = True
                 cam.solver.set_stream(st)
                 key = (cam.height, cam.width)
-                hi0, hi1, hu = self._staging(lane, cam.height, cam.width, used[key])
+                hi0, hi1, hu, di0, di1, du = self._staging(lane, cam.height, cam.width, used[key])
                 used[key] += 1
                 np.copyto(hi0.numpy(), r.i0)
                 np.copyto(hi1.numpy(), r.i1)
-                ins.append((hi0.to(self.device, non_blocking=True), hi1.to(self.device, non_blocking=True)))
-                outs.append(torch.empty((cam.height, cam.width), dtype=torch.float32, device=self.device))
+                di0.copy_(hi0, non_blocking=True)
+                di1.copy_(hi1, non_blocking=True)
+                ins.append((di0, di1))
+                outs.append(du)
                 hosts.append(hu)
                 if self.path != "plain":
                     lane.batch.add(cam.solver)
