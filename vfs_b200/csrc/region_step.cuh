@@ -98,14 +98,6 @@ struct RegionState {
   // Dual step and T p at region pixel i of image pixel (gx, gy) inside the image.  Returns
   // false for a masked-out pixel of the masked form (it keeps its values; its stored T p is
   // in tp).
-  // a pixel whose code (and, for the plain form, position) makes every edge rule take its
-  // interior branch: on, with the four neighbours in the image (and, masked, on)
-  template <bool MASKED>
-  static __device__ __forceinline__ bool interior(uint8_t cd, int gx, int gy, int w, int h) {
-    if (MASKED) return cd == (kOn | kR | kL | kD | kU);
-    return (cd & kOn) && gx >= 1 && gy >= 1 && gx + 1 < w && gy + 1 < h;
-  }
-
   template <bool MASKED>
   __device__ __forceinline__ bool dual(int i, int RX, int gx, int gy, int w, int h, float sp, float sq) {
     typedef Store2<ST> S;
@@ -113,17 +105,6 @@ struct RegionState {
     const uint8_t cd = code[i];
     bool useRight, useDown;
     const float a_ = a[i], b_ = b[i], c_ = c[i];
-    if (kFast && interior<MASKED>(cd, gx, gy, w, h)) {
-      // the right / down neighbours, no edge rule: the packed form of the same operations
-      float2 pp = S::cvt2(p[i]);
-      float4 qq = S::cvt4(S::rnd4(q[i]));
-      fast::dual_interior(ub[i], ub[i + 1], ub[i + RX], S::cvt2(v[i]), S::cvt2(v[i + 1]), S::cvt2(v[i + RX]), a_, b_,
-                          c_, sp, sq, pp, qq);
-      p[i] = S::rnd2(pp);
-      q[i] = qq;
-      tp[i] = fast::tp(a_, b_, c_, pp);
-      return true;
-    }
     if (MASKED) {
       if (!(cd & kOn)) return false;
       useRight = cd & kR;
@@ -172,24 +153,6 @@ struct RegionState {
     float dxm, dym;
     bool zR, zD, hasL, hasU;
     const float2 t = tp[i], tpW = tp[i - 1], tpN = tp[i - RX];
-    if (kFast && interior<MASKED>(cd, gx, gy, w, h)) {
-      // central differences, no edge rule: the packed form of the same operations
-      const float a_ = a[i], b_ = b[i], c_ = c[i];
-      const float ubar = ub[i];
-      const float2 vb = S::cvt2(v[i]);
-      const float eu = fast::etau(a_, b_, c_, P.alpha1 * P.alpha1);
-      const float unew = fast::threshold(t.x - tpW.x, t.y - tpN.y, eu, tau, ubar, u[i], Iu[i], Iz[i], P.lambda);
-      const float4 ql = q[i - 1], qu = q[i - RX];
-      const float a1s = P.alpha1 * P.alpha1, a0s4 = 4.0f * P.alpha0 * P.alpha0;
-      float us_;
-      float2 vs;
-      fast::primal_interior(q[i], make_float2(ql.x, ql.w), make_float2(qu.z, qu.y), t, fast::etav(b_, c_, a1s, a0s4),
-                            fast::etav(a_, c_, a1s, a0s4), tau, P.alpha0, P.alpha1, mu, vb, unew, ubar, us_, vs);
-      u[i] = unew;
-      ub[i] = us_;
-      v[i] = S::rnd2(vs);
-      return;
-    }
     if (MASKED) {
       const bool mR = cd & kR, mL = cd & kL, mD = cd & kD, mU = cd & kU;
       if (mL && mR) dxm = t.x - tpW.x;
