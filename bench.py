@@ -390,19 +390,14 @@ def run_ours(args, rank, world, local):
             s.solveStereoForwardMasked()
             s.copy_1d_disparity_to_device(o)
 
-    # Profiling records are part of the captured graphs: enable them before the warm-up so
-    # that no graph is captured inside the timed region.
-    for s in solvers:
-        s.profile(True)
+    # The timed region runs without the per-level profiling records (CUDA events inside the
+    # captured graphs, which cost about 3 % of a step); its graphs are captured in the warm-up.
     for _ in range(args.warmup):
         device_step()
         flush.fill_(1.0)
     torch.cuda.synchronize()
 
     # ---- timed region: device-resident inputs -----------------------------------------
-    for s in solvers:
-        s.profile_reset()
-    StereoTgv.profile_epoch(stream)
     launches0 = StereoTgv.launch_count()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if world > 1:
@@ -422,6 +417,23 @@ def run_ours(args, rank, world, local):
     launches = StereoTgv.launch_count() - launches0
     step_ms = [a.elapsed_time(b) for a, b in ev]
     total_ms = float(sum(step_ms))
+    # ---- roofline pass (not timed into the value): the same steps with the per-level
+    # profiling records, whose graphs are captured by two untimed steps first
+    for s in solvers:
+        s.profile(True)
+    for _ in range(2):
+        device_step()
+        flush.fill_(1.0)
+    torch.cuda.synchronize()
+    for s in solvers:
+        s.profile_reset()
+    StereoTgv.profile_epoch(stream)
+    n_prof = max(1, min(args.steps, 5))
+    for k in range(n_prof):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+        device_step()
+    torch.cuda.synchronize()
     # roofline of the inner primal-dual loop: kind 0 (drop-in, one record per iteration)
     # Pairs solved on concurrent streams overlap, so the time is the union of the records'
     # intervals (time during which at least one inner group ran), not their sum.
@@ -530,7 +542,8 @@ def run_ours(args, rank, world, local):
                          "algorithmic_bytes_per_launch": b_alg * px_per_launch,
                          "bytes_per_pixel_iteration": b_alg, "peak_kind": peak_kind,
                          "time_basis": "union of the full-resolution inner-loop event intervals of all pairs "
-                                       "in the last timed step (concurrent pairs overlap)",
+                                       "in the last step of a profiled pass run after the timed region on the "
+                                       "same inputs (concurrent pairs overlap)",
                          "busy_ms": ms_l, "sum_of_interval_ms": ms_sum,
                          "all_levels": {"achieved": achieved_all, "frac": (achieved_all / peak) if achieved_all else None,
                                         "busy_ms": ms_all},
