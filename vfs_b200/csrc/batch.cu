@@ -129,6 +129,10 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
         d.beta = s->P.beta;
         d.gamma = s->P.gamma;
         d.cuda_math = s->tensor_cuda_math;
+        d.abce = half ? s->f_abce : nullptr;
+        d.rv = half ? s->f_rv : nullptr;
+        d.alpha0 = s->P.alpha0;
+        d.alpha1 = s->P.alpha1;
         set_tiles(L, k, d.w, d.h);
       }
       L.npairs = na;
@@ -200,6 +204,8 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
           d.c = s->d_c;
           d.Iu = s->d_Iu;
           d.Iz = s->d_Iz;
+          d.abce = half ? s->f_abce : nullptr;
+          d.rv = half ? s->f_rv : nullptr;
           d.us = s->d_us;
           d.u_s = s->d_u_s;
           d.v_s = half ? s->f_vhs : (void*)s->d_v_s;

@@ -97,6 +97,10 @@ struct IterPair {
   void* q;              // T4, in place
   float2* Tp;           // T p (float); read for masked-out neighbours, written when write_tp
   const float *a, *b, *c, *Iu, *Iz;
+  // half storage: the level's coefficient records (k_level_tensor), read by k_fused_iter in
+  // place of a, b, c: (a, b, c, etau_rcp) and etav_rcp (tgv_pixel_fast.cuh); null otherwise
+  const float4* abce;
+  const float2* rv;
   float* us;            // thresholded u (output)
   float* u_s;           // new u-bar (output)
   void* v_s;            // new v-bar (output), T2
@@ -233,6 +237,11 @@ struct LevelPair {
   int w, h, s, xmax, tiles_x, tile0;
   float beta, gamma;
   int cuda_math;  // tensor weight from CUDA's expf / powf (1) or the portable construction (0)
+  // half storage: also write the coefficient records of the iteration (IterPair::abce / rv),
+  // whose reciprocal preconditioners take alpha0 and alpha1; null otherwise
+  float4* abce;
+  float2* rv;
+  float alpha0, alpha1;
 };
 struct LevelArgs {
   int npairs, ntiles;

@@ -182,11 +182,22 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   uint8_t code = 0;
   float a = 0.f, b = 0.f, c = 0.f, ubar = 0.f;
   float u_th = 0.f, Iu_th = 0.f, Iz_th = 0.f;
+  // half storage: the reciprocal preconditioners come with a, b, c from the level's records
+  float r_eu = 0.f;
+  float2 r_ev = make_float2(0.f, 0.f);
   if (in_img) {
     if (!blk_inner) code = P.code[pos];
-    a = P.a[pos];
-    b = P.b[pos];
-    c = P.c[pos];
+    if (kFast) {
+      const float4 r = P.abce[pos];
+      a = r.x;
+      b = r.y;
+      c = r.z;
+      r_eu = r.w;
+    } else {
+      a = P.a[pos];
+      b = P.b[pos];
+      c = P.c[pos];
+    }
   }
   // masked form: a block with no pixel on in its region writes nothing and reads nothing
   // another block needs, so it leaves here.  With tile spans the grid holds only tiles
@@ -227,6 +238,9 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   sQzy[ry][rx] = make_float2(qq.z, qq.y);
   __syncthreads();
   if (!tile || !in_img) return;
+  // read here rather than with the phase-1 loads, where holding it across the barrier costs
+  // registers; its latency overlaps the threshold step
+  if (kFast) r_ev = P.rv[pos];
 
   // ---- phase 2: thresholding --------------------------------------------------------
   float dxm, dym;
@@ -269,8 +283,7 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   }
   float unew;
   if (kFast) {
-    float eu = fast::etau(a, b, c, P.alpha1 * P.alpha1);
-    unew = fast::threshold(dxm, dym, eu, A.tau, ubar, u_th, Iu_th, Iz_th, P.lambda);
+    unew = fast::threshold_teu(dxm, dym, A.tau * r_eu, ubar, u_th, Iu_th, Iz_th, P.lambda);
   } else {
     float eu = etau_math(a, b, c, P.alpha1);
     unew = threshold_math(dxm, dym, eu, A.tau, ubar, u_th, Iu_th, Iz_th, P.lambda);
@@ -287,12 +300,10 @@ __global__ void __launch_bounds__(32 * (TH + 1), MINB) k_fused_iter(const __grid
   float us_;
   float2 vs;
   if (kFast) {
-    const float a1s = P.alpha1 * P.alpha1, a0s4 = 4.0f * P.alpha0 * P.alpha0;
-    float ev1 = fast::etav(b, c, a1s, a0s4), ev2 = fast::etav(a, c, a1s, a0s4);
     if (inner)
-      fast::primal_interior(qq, qxw_l, qzy_u, tp, ev1, ev2, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs);
+      fast::primal_interior_r(qq, qxw_l, qzy_u, tp, r_ev, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs);
     else
-      fast::primal(qc, ql, qu, tp, ev1, ev2, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs);
+      fast::primal_r(qc, ql, qu, tp, r_ev, A.tau, P.alpha0, P.alpha1, A.mu, vb, unew, ubar, us_, vs);
   } else {
     float ev1 = etav1_math(b, c, P.alpha0, P.alpha1), ev2 = etav2_math(a, c, P.alpha0, P.alpha1);
     float2 vo;
@@ -508,6 +519,16 @@ __global__ void __launch_bounds__(kFTW* kFTH) k_level_gaussian(const __grid_cons
   P.i0smooth[pos] = t0;
 }
 
+// The half-storage iteration's per-level records at one pixel: (a, b, c, 1 / eta_u) and
+// (1 / eta_v1, 1 / eta_v2), formed by the same expressions the iteration kernels use
+// (tgv_pixel_fast.cuh, a1s = alpha1^2, a0s4 = 4 alpha0^2), so reading them gives the bits of
+// recomputing them.
+__device__ __forceinline__ void level_records(const LevelPair& P, long long pos, float a, float b, float c) {
+  const float a1s = P.alpha1 * P.alpha1, a0s4 = 4.0f * P.alpha0 * P.alpha0;
+  P.abce[pos] = make_float4(a, b, c, fast::etau_rcp(fast::etau(a, b, c, a1s)));
+  P.rv[pos] = fast::etav_rcp(fast::etav(b, c, a1s, a0s4), fast::etav(a, c, a1s, a0s4));
+}
+
 // calcTensor.cu:8-73 / 155-219; a = b = c = 0 where the reference does not compute
 // (masked out, or columns >= xmax of its launch grid)
 __global__ void __launch_bounds__(kFTW* kFTH) k_level_tensor(const __grid_constant__ LevelArgs A) {
@@ -518,6 +539,7 @@ __global__ void __launch_bounds__(kFTW* kFTH) k_level_tensor(const __grid_consta
     P.a[pos] = 0.0f;
     P.b[pos] = 0.0f;
     P.c[pos] = 0.0f;
+    if (P.abce) level_records(P, pos, 0.0f, 0.0f, 0.0f);
     return;
   }
   float dx = 1.0f / (float)P.w, dy = 1.0f / (float)P.h;
@@ -535,9 +557,11 @@ __global__ void __launch_bounds__(kFTW* kFTH) k_level_tensor(const __grid_consta
   float ntx = ny, nty = -nx;
   float wt = tensor_weight(abs_img, P.beta, P.gamma, P.cuda_math);
   if (!(wt > 1e-8f)) wt = 1e-8f;
-  P.a[pos] = wt * nx * nx + ntx * ntx;
-  P.c[pos] = wt * nx * ny + ntx * nty;
-  P.b[pos] = wt * ny * ny + nty * nty;
+  const float a = wt * nx * nx + ntx * ntx, c = wt * nx * ny + ntx * nty, b = wt * ny * ny + nty * nty;
+  P.a[pos] = a;
+  P.c[pos] = c;
+  P.b[pos] = b;
+  if (P.abce) level_records(P, pos, a, b, c);
 }
 
 void launch_level_gaussian(const LevelArgs& A, cudaStream_t st) {

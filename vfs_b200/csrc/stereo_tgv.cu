@@ -127,6 +127,8 @@ void StereoTgvImpl::release() {
   if (fpool_) cudaFree(fpool_);
   fpool_ = nullptr;
   f_p = f_q = f_vh = f_vhs = nullptr;
+  f_abce = nullptr;
+  f_rv = nullptr;
   code_masked.clear();
   code_plain.clear();
   codes_valid = false;
@@ -159,7 +161,7 @@ static size_t pool_bytes_for(const std::vector<int>& pS, const std::vector<int>&
 // p, q two planes each (float: 8 + 16 bytes per pixel and plane), half v-bar pair, and
 // two edge-code bytes per pixel and level.
 static size_t fused_bytes_for(const std::vector<int>& pS, const std::vector<int>& pH, size_t full) {
-  size_t bytes = full * 2 * 8 + full * 2 * 16 + full * 4 * 2 + 8 * 512;
+  size_t bytes = full * 2 * 8 + full * 2 * 16 + full * 4 * 2 + full * 16 + full * 8 + 8 * 512;
   for (size_t l = 0; l < pS.size(); l++) bytes += 2 * ((size_t)pS[l] * pH[l] + 512);
   return bytes;
 }
@@ -399,6 +401,8 @@ void StereoTgvImpl::ensureFused() {
   f_q = take(n * 2 * 16);
   f_vh = take(n * 4);
   f_vhs = take(n * 4);
+  f_abce = (float4*)take(n * 16);
+  f_rv = (float2*)take(n * 8);
   code_masked.assign(levels(), nullptr);
   code_plain.assign(levels(), nullptr);
   for (int l = 0; l < levels(); l++) {

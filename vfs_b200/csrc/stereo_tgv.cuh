@@ -168,6 +168,9 @@ class StereoTgvImpl {
   void* f_q = nullptr;
   void* f_vh = nullptr;  // current half v-bar
   void* f_vhs = nullptr; // other half v-bar
+  // half storage: the current level's coefficient records of the iteration (IterPair::abce, rv)
+  float4* f_abce = nullptr;
+  float2* f_rv = nullptr;
   std::vector<uint8_t*> code_masked, code_plain;
   bool codes_valid = false;
   // per level: the K-iterations-per-launch kernel reproduces the masked form exactly (false

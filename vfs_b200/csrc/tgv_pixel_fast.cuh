@@ -153,11 +153,24 @@ __device__ __forceinline__ float etav(float x, float c, float a1s, float a0s4) {
   return __fmaf_rn(a1s, __fmaf_rn(x, x, c * c), a0s4);
 }
 
-// L1 thresholding (the three cases of the linearised data term).
-__device__ __forceinline__ float threshold(float dxm, float dym, float eu, float tau, float u_bar, float upos,
-                                           float Ius, float Iz, float lambda) {
+// Reciprocal preconditioners, constant over a pyramid level (a, b, c are): the fused
+// iteration takes them from a per-level record (k_level_tensor) instead of recomputing them
+// every iteration.  Each is the value the step would form itself, so the result is the same
+// bit for bit either way.
+//   etau_rcp: 1 / eta_u, or 1 where eta_u = 0 (the step is then tau itself: tau * 1 = tau).
+//   etav_rcp: (1 / eta_v1, or 1 where eta_v1 = 0; 1 / eta_v2, or -0 where eta_v2 = 0).  eta_v2
+//   is a sum of non-negative terms (or NaN), so rcp never gives -0 for it and -0 marks the
+//   eta_v2 = 0 branch of updatePrimalVariables.cu:103-105 unambiguously.
+__device__ __forceinline__ float etau_rcp(float eu) { return (eu == 0.0f) ? 1.0f : rcp(eu); }
+__device__ __forceinline__ float2 etav_rcp(float ev1, float ev2) {
+  return make_float2(ev1 != 0.0f ? rcp(ev1) : 1.0f, ev2 != 0.0f ? rcp(ev2) : -0.0f);
+}
+__device__ __forceinline__ bool etav2_zero(float r2) { return __float_as_uint(r2) == 0x80000000u; }
+
+// L1 thresholding (the three cases of the linearised data term); teu = tau / eta_u.
+__device__ __forceinline__ float threshold_teu(float dxm, float dym, float teu, float u_bar, float upos, float Ius,
+                                               float Iz, float lambda) {
   float div_p = dxm + dym;
-  float teu = (eu == 0.0f) ? tau : tau * rcp(eu);
   float dun = __fmaf_rn(teu, div_p, u_bar) - upos;
   float rho = __fmaf_rn(Ius, dun, Iz);
   float lt = lambda * teu;
@@ -172,37 +185,52 @@ __device__ __forceinline__ float threshold(float dxm, float dym, float eu, float
   }
   return upos + d;
 }
+__device__ __forceinline__ float threshold(float dxm, float dym, float eu, float tau, float u_bar, float upos,
+                                           float Ius, float Iz, float lambda) {
+  return threshold_teu(dxm, dym, tau * etau_rcp(eu), u_bar, upos, Ius, Iz, lambda);
+}
 
 // Primal update with the x / y lanes paired: dq = (q.x - ql.x) + (q.z - qu.z) and
 // (q.w - ql.w) + (q.y - qu.y), g = alpha1 T p + alpha0 dq, v = v-bar + (tau / eta_v) g (the
 // eta_v2 = 0 case of updatePrimalVariables.cu:103-105 writes .x again and keeps .y), then the
 // over-relaxation.  qxw_l = (q.x, q.w) of the west neighbour, qzy_u = (q.z, q.y) of the north
 // one (zero where absent).
-__device__ __forceinline__ void primal_interior(float4 qc, float2 qxw_l, float2 qzy_u, float2 tpp, float ev1,
-                                                float ev2, float tau, float alpha0, float alpha1, float mu, float2 vb,
-                                                float u_new, float u_bar, float& u_s, float2& v_s) {
+// r12 = etav_rcp(eta_v1, eta_v2).
+__device__ __forceinline__ void primal_interior_r(float4 qc, float2 qxw_l, float2 qzy_u, float2 tpp, float2 r12,
+                                                  float tau, float alpha0, float alpha1, float mu, float2 vb,
+                                                  float u_new, float u_bar, float& u_s, float2& v_s) {
   using namespace x2;
   const f2 dq = add(sub(pk(qc.x, qc.w), pk(qxw_l.x, qxw_l.y)), sub(pk(qc.z, qc.y), pk(qzy_u.x, qzy_u.y)));
   const f2 g = fma(pk(alpha1, alpha1), pk(tpp.x, tpp.y), mul(pk(alpha0, alpha0), dq));
   const f2 vbb = pk(vb.x, vb.y);
   f2 v;
-  if (ev2 != 0.0f) {
-    v = fma(pk(ev1 != 0.0f ? tau * rcp(ev1) : tau, tau * rcp(ev2)), g, vbb);
+  if (!etav2_zero(r12.y)) {
+    v = fma(pk(tau * r12.x, tau * r12.y), g, vbb);
   } else {  // updatePrimalVariables.cu:103-105 writes .x again; .y keeps the previous value
     v = pk(__fmaf_rn(tau, upk(g).x, vb.x), vb.y);
   }
   u_s = __fmaf_rn(mu, u_new - u_bar, u_new);
   v_s = upk(fma(pk(mu, mu), sub(v, vbb), v));
 }
+__device__ __forceinline__ void primal_interior(float4 qc, float2 qxw_l, float2 qzy_u, float2 tpp, float ev1,
+                                                float ev2, float tau, float alpha0, float alpha1, float mu, float2 vb,
+                                                float u_new, float u_bar, float& u_s, float2& v_s) {
+  primal_interior_r(qc, qxw_l, qzy_u, tpp, etav_rcp(ev1, ev2), tau, alpha0, alpha1, mu, vb, u_new, u_bar, u_s, v_s);
+}
 
 
 // Primal update of v and the over-relaxation of u and v; tpp = T p at this pixel; ql / qu: q
 // of the west / north neighbour (zero where absent), of which the step reads (x, w) / (z, y).
+__device__ __forceinline__ void primal_r(float4 qc, float4 ql, float4 qu, float2 tpp, float2 r12, float tau,
+                                         float alpha0, float alpha1, float mu, float2 vb, float u_new, float u_bar,
+                                         float& u_s, float2& v_s) {
+  primal_interior_r(qc, make_float2(ql.x, ql.w), make_float2(qu.z, qu.y), tpp, r12, tau, alpha0, alpha1, mu, vb,
+                    u_new, u_bar, u_s, v_s);
+}
 __device__ __forceinline__ void primal(float4 qc, float4 ql, float4 qu, float2 tpp, float ev1, float ev2, float tau,
                                        float alpha0, float alpha1, float mu, float2 vb, float u_new, float u_bar,
                                        float& u_s, float2& v_s) {
-  primal_interior(qc, make_float2(ql.x, ql.w), make_float2(qu.z, qu.y), tpp, ev1, ev2, tau, alpha0, alpha1, mu, vb,
-                  u_new, u_bar, u_s, v_s);
+  primal_r(qc, ql, qu, tpp, etav_rcp(ev1, ev2), tau, alpha0, alpha1, mu, vb, u_new, u_bar, u_s, v_s);
 }
 
 }  // namespace fast
