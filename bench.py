@@ -572,7 +572,7 @@ def run_ours(args, rank, world, local):
             result["mixed_batch"] = {k: mixed[k] for k in ("value", "unit", "ms_per_step", "latency_ms",
                                                             "max_abs_vs_plain_px", "one_launch_per_level",
                                                             "config")}
-            srv = run_serving(args, emit=False)
+            srv = run_serving(args, emit=False, local=local)
             result["serving"] = dict(srv["serving"], config=srv["config"])
             result["warm_start"] = warm_start_report(args.seed)
         print(json.dumps(result), flush=True)
@@ -723,23 +723,39 @@ def warm_start_report(seed, n_frames=8, width=424, height=400):
     return out
 
 
-def run_serving(args, emit=True):
+def run_serving(args, emit=True, rank=0, world=1, local=0):
     """6 camera streams (4 x 848x800, 2 x 424x400), 120 frames each along smooth random
     trajectories, Poisson arrivals totalling 180 requests/s, served by the continuous-batching
-    server (fused, FP16 storage) and by the drop-in path one request at a time."""
+    server (fused, FP16 storage) and by the drop-in path one request at a time.  Under torchrun
+    each rank serves the streams `replicas.assign_streams` gives it on its own GPU (the streams
+    are independent) and rank 0 reports the job: all requests' latencies, all frames over the
+    span from the first arrival to the last completion on any rank."""
     import torch
     from vfs_b200 import synth
     from vfs_b200.build import build
+    from vfs_b200.replicas import merge_serving, my_streams
     from vfs_b200.serving import StereoServer, poisson_schedule, replay
-    build()
+    torch.cuda.set_device(local)
+    if rank == 0:
+        build()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.barrier()
+        build()
     n_frames = max(8, min(120, args.steps * 12))
-    cams = [(0, 848, 800), (1, 848, 800), (2, 848, 800), (3, 848, 800), (4, 424, 400), (5, 424, 400)]
+    cams_all = [(0, 848, 800), (1, 848, 800), (2, 848, 800), (3, 848, 800), (4, 424, 400), (5, 424, 400)]
+    owned = set(my_streams({sid: (w, h) for sid, w, h in cams_all}, world, rank))
+    cams = [c for c in cams_all if c[0] in owned]
     data = {}
     for sid, w, h in cams:
         fields, frames = synth.make_sequence_gpu(w, h, args.seed + 7 * sid, n_frames)
         data[sid] = (w, h, fields, frames)
-    rates = {sid: 30.0 for sid, _, _ in cams}
-    sched = poisson_schedule(rates, {sid: n_frames for sid, _, _ in cams}, seed=args.seed)
+    # one schedule for the whole job (every rank draws the same one), each rank replays its part
+    rates = {sid: 30.0 for sid, _, _ in cams_all}
+    sched = poisson_schedule(rates, {sid: n_frames for sid, _, _ in cams_all}, seed=args.seed)
+    sched = [ev for ev in sched if ev[1] in owned]
     sp = synth.SOLVER_PARAMS
     params = dict(sp, limitRange=synth.LIMIT_RANGE)
     out = {}
@@ -755,20 +771,31 @@ def run_serving(args, emit=True):
                 srv.submit(sid, *frames[0])
             srv.run_until_idle()
         srv.done.clear()
+        if world > 1:
+            torch.distributed.barrier()  # the ranks start their replays together
         t_start = time.perf_counter()
         replay(srv, sched, {sid: d[3] for sid, d in data.items()}, realtime=True)
         st = srv.stats(since=t_start)
+        if world > 1:
+            d = [r for r in srv.done if r.t_submit >= t_start]
+            job = merge_serving([r.latency_ms for r in d], min((r.t_submit for r in d), default=0.0),
+                                max((r.t_done for r in d), default=0.0))
+            st = dict(st, **job)
         st["arrival_rate_per_s"] = 180.0
         out[label] = st
         del srv
         torch.cuda.synchronize()
     line = {"metric": "serving: 6 camera streams, 180 requests/s Poisson, p50/p99 latency and frames/s",
-            "value": out["fused_fp16_batched"].get("frames_per_s"), "unit": "frames/s", "n_gpus": 1,
+            "value": out["fused_fp16_batched"].get("frames_per_s"), "unit": "frames/s", "n_gpus": world,
             "higher_is_better": True, "data": "synthetic",
-            "config": {"workload": "4 x 848x800 + 2 x 424x400 streams, %d frames each, 30 req/s each" % n_frames},
+            "config": {"workload": "4 x 848x800 + 2 x 424x400 streams, %d frames each, 30 req/s each" % n_frames,
+                       "parallelism": "replicas x%d (streams assigned to ranks by pixels per frame)" % world},
             "serving": out}
-    if emit:
+    if emit and rank == 0:
         print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
     return line
 
 
@@ -783,8 +810,7 @@ def main():
             run_mixed(args)
         return
     if args.mode == "serving":
-        if rank == 0:
-            run_serving(args)
+        run_serving(args, rank=rank, world=world, local=local)
         return
     run_ours(args, rank, world, local)
 

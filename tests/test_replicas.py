@@ -71,3 +71,52 @@ def test_job_rate_over_two_gloo_ranks():
         assert abs(rate - 16 / 0.015) < 1e-6
     assert sorted(res[0][4] + res[1][4]) == sorted(STREAMS)
     assert not set(res[0][4]) & set(res[1][4])
+
+
+def _serving_rank(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    from vfs_b200.replicas import merge_serving
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        # rank 0 served 3 requests from t = 1.0 s to 2.0 s, rank 1 one request from 1.5 s to 3.0 s
+        lat = [10.0, 20.0, 30.0] if rank == 0 else [40.0]
+        span = (1.0, 2.0) if rank == 0 else (1.5, 3.0)
+        q.put((rank, merge_serving(lat, *span)))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.timeout(120)
+def test_serving_figures_merge_over_two_gloo_ranks():
+    """Multi-GPU serving: every rank reports the job's figures over all ranks' requests."""
+    import numpy as np
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_serving_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=90) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for _, st in res:
+        assert st["frames"] == 4
+        assert abs(st["frames_per_s"] - 4 / 2.0) < 1e-9  # first arrival 1.0 s, last completion 3.0 s
+        assert abs(st["p50_ms"] - float(np.percentile([10, 20, 30, 40], 50))) < 1e-9
+        assert abs(st["p99_ms"] - float(np.percentile([10, 20, 30, 40], 99))) < 1e-9
+    assert res[0][1] == res[1][1]
+
+
+def test_serving_merge_without_process_group_is_local():
+    from vfs_b200.replicas import merge_serving
+    st = merge_serving([5.0, 7.0], 0.0, 0.5)
+    assert st["frames"] == 2 and abs(st["frames_per_s"] - 4.0) < 1e-9 and st["mean_ms"] == 6.0
+    assert merge_serving([], 0.0, 0.0) == {"frames": 0}

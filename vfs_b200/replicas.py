@@ -52,3 +52,25 @@ def job_rate(frames_local: float, ms_local: float, device=None):
         dist.all_reduce(m, op=dist.ReduceOp.MAX)
         frames, ms = float(f.item()), float(m.item())
     return frames, ms, (frames / (ms / 1000.0) if ms > 0 else 0.0)
+
+
+def merge_serving(latencies_ms: List[float], t_first: float, t_last: float) -> dict:
+    """Job-wide serving figures over ranks: every rank's request latencies (ms) and the span
+    from the earliest arrival to the latest completion on any rank (time.perf_counter seconds:
+    one host's monotonic clock, so comparable between its processes).  Without an initialized
+    process group these are the local figures."""
+    import numpy as np
+    import torch.distributed as dist
+
+    parts = [(list(latencies_ms), float(t_first), float(t_last))]
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        parts = [None] * dist.get_world_size()
+        dist.all_gather_object(parts, (list(latencies_ms), float(t_first), float(t_last)))
+    lat = np.array([x for p in parts for x in p[0]], dtype=np.float64)
+    if lat.size == 0:
+        return {"frames": 0}
+    busy = [p for p in parts if p[0]]
+    span = max(p[2] for p in busy) - min(p[1] for p in busy)
+    return {"frames": int(lat.size), "frames_per_s": float(lat.size / span) if span > 0 else None,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean())}
