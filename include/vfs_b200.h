@@ -225,7 +225,9 @@ int vfs_batch_set_fine_concurrency(vfs_batch* b, int max_pairs);
  * pairs at a time (pair k's after pair k - max_pairs's); priority = 1 runs the
  * full-resolution parts on high-priority streams, priority = 2 also the first max_pairs
  * pairs' coarser levels, so that full-resolution work starts while the other pairs' coarse
- * levels run.  Results are unchanged. */
+ * levels run; priority = 3 runs all of pair k's work at the priority of its full-resolution
+ * round k / max_pairs (the first round highest), so that each round's coarse levels fill the
+ * gaps of the rounds before it.  Results are unchanged. */
 int vfs_batch_set_pipeline(vfs_batch* b, int stagger_coarse, int priority);
 int vfs_set_autotune(vfs_stereo* s, int on);
 /* Force one variant of the fused iteration kernel at every pyramid level (-1: the tuned or

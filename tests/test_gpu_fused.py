@@ -319,11 +319,12 @@ def test_retired_variants_are_rejected(gpu):
     s.set_iteration_variant(-1)  # back to the tuner
 
 
-@pytest.mark.parametrize("fine,stagger,prio", [(1, 0, 0), (2, 0, 2), (2, 1, 1), (3, 1, 0)])
+@pytest.mark.parametrize("fine,stagger,prio", [(1, 0, 0), (2, 0, 2), (2, 1, 1), (3, 1, 0), (2, 0, 3), (1, 0, 3), (2, 0, 4)])
 def test_fine_concurrency_limit_keeps_results(gpu, fine, stagger, prio):
     """Splitting each pair's solve into coarse levels and a full-resolution part, with at most
     `fine` pairs at full resolution at a time (optionally with the coarse parts staggered the
-    same way and the full-resolution parts on high-priority streams), gives the same bits as
+    same way, the full-resolution parts on high-priority streams, or every part at the priority
+    of its full-resolution round), gives the same bits as
     the unsplit batch, over two frames and from host buffers too."""
     from vfs_b200.stereotgv import StereoBatch
     cases = [(96, 64, 2), (130, 101, 3), (67, 53, 2), (200, 120, 3)]

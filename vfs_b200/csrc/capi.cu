@@ -3,6 +3,7 @@
 // message on the handle; nothing here exits the process.
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <new>
 #include <string>
 
@@ -26,8 +27,11 @@ struct vfs_batch {
   std::vector<cudaStream_t> fine_lanes;  // concurrent mode: streams of the full-resolution parts
   int fine_limit = -1;  // concurrent mode: pairs at full resolution at once (0: no limit, -1: auto)
   bool stagger_coarse = false;  // coarse parts also S at a time, one slot ahead of the fine parts
-  int fine_priority = 0;  // 1: full-resolution parts on high-priority streams; 2: also the
-                          // coarse parts of the first max_pairs pairs
+  int fine_priority = 4;  // 0: no priorities; 1: full-resolution parts on high-priority
+                          // streams; 2: also the coarse parts of the first max_pairs pairs; 3:
+                          // every part of pair k at the priority of its full-resolution round
+                          // k / max_pairs; 4 (default): coarse parts above full-resolution parts
+  std::map<int, std::vector<cudaStream_t>> graded_lanes;  // priority 3: per priority, one stream per slot
   int mode = VFS_BATCH_CONCURRENT;
   bool half = false;
   std::string err;
@@ -38,6 +42,8 @@ struct vfs_batch {
     for (auto e : fine_done) cudaEventDestroy(e);
     for (auto e : coarse_done) cudaEventDestroy(e);
     for (auto l : fine_lanes) cudaStreamDestroy(l);
+    for (auto& g : graded_lanes)
+      for (auto l : g.second) cudaStreamDestroy(l);
     for (auto l : lanes) cudaStreamDestroy(l);
     if (done) cudaEventDestroy(done);
     if (start) cudaEventDestroy(start);
@@ -441,7 +447,7 @@ int vfs_batch_set_fine_concurrency(vfs_batch* b, int max_pairs) {
 
 int vfs_batch_set_pipeline(vfs_batch* b, int stagger_coarse, int priority) {
   return guarded(b, [&] {
-    if (priority < 0 || priority > 2) throw vfs::ArgError{"pipeline priority must be 0, 1 or 2"};
+    if (priority < 0 || priority > 4) throw vfs::ArgError{"pipeline priority must be 0 to 4"};
     b->stagger_coarse = stagger_coarse != 0;
     b->fine_priority = priority;
   });
@@ -533,12 +539,34 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
     const bool split = S > 0 && S < n;
     int prio_lo = 0, prio_hi = 0;
     VFS_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-    auto run = [&](int k, int part, int concurrency, cudaStream_t lane, bool high = false) {
-      struct PrioScope {  // the launches of this part carry the high priority
+    // priority 3: pair k's coarse and full-resolution parts run at the priority of its
+    // full-resolution round k / S (round 0 the highest), so that the GPU prefers the work of the
+    // earliest round and the later rounds' coarse levels fill the gaps its launches leave
+    // priority 4: the coarse parts, latency-bound chains of small launches, run above the
+    // full-resolution parts (the first round's coarse parts highest), so that every pair's
+    // chain advances at its own pace and the full-resolution launches fill the rest of the GPU
+    const bool graded = split && (b->fine_priority == 3 || b->fine_priority == 4);
+    const bool coarse_first = b->fine_priority == 4;
+    auto round_prio = [&](int k) {
+      if (coarse_first) return std::min(prio_lo, prio_hi + (k < S ? 0 : 1));
+      return std::min(prio_lo, prio_hi + k / S);
+    };
+    auto graded_lane = [&](int k) -> cudaStream_t {
+      std::vector<cudaStream_t>& v = b->graded_lanes[round_prio(k)];
+      while ((int)v.size() <= k) {
+        cudaStream_t l;
+        VFS_CUDA(cudaStreamCreateWithPriority(&l, cudaStreamNonBlocking, round_prio(k)));
+        v.push_back(l);
+      }
+      return v[k];
+    };
+    // prio: the priority the launches of this part carry (0: none)
+    auto run = [&](int k, int part, int concurrency, cudaStream_t lane, int prio = 0) {
+      struct PrioScope {
         int old;
         PrioScope(int p) : old(vfs::launch_priority()) { vfs::launch_priority() = p; }
         ~PrioScope() { vfs::launch_priority() = old; }
-      } prio_scope(high ? prio_hi : 0);
+      } prio_scope(prio);
       std::vector<vfs::StereoTgvImpl*> one{pairs[k]};
       vfs::FusedEngine& eng = pairs[k]->engine;
       const bool g = eng.use_graph, t = eng.autotune;
@@ -571,12 +599,13 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
       if (split && b->stagger_coarse && k >= S) VFS_CUDA(cudaStreamWaitEvent(b->lanes[k], b->coarse_done[k - S], 0));
       // the first S pairs' coarse parts on the high-priority streams (their full-resolution
       // parts follow there), so that full-resolution work starts early
-      cudaStream_t cl = (split && b->fine_priority >= 2 && k < S) ? b->fine_lanes[k] : b->lanes[k];
+      cudaStream_t cl = graded ? graded_lane(k)
+                               : (split && b->fine_priority >= 2 && k < S) ? b->fine_lanes[k] : b->lanes[k];
       if (cl != b->lanes[k]) VFS_CUDA(cudaStreamWaitEvent(cl, b->start, 0));
       if (io)
         pairs[k]->copyImagesU8On(io->i0[k], io->i1[k], io->device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
                                  cl);
-      run(k, split ? 1 : 0, n, cl, cl != b->lanes[k]);
+      run(k, split ? 1 : 0, n, cl, graded ? round_prio(k) : cl != b->lanes[k] ? prio_hi : 0);
       if (split) {
         VFS_CUDA(cudaEventRecord(b->coarse_done[k], cl));
         continue;
@@ -588,10 +617,12 @@ void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
     }
     if (split) {
       for (int k = 0; k < n; k++) {
-        cudaStream_t fl = b->fine_priority ? b->fine_lanes[k] : b->lanes[k];
+        cudaStream_t fl = coarse_first ? b->lanes[k]
+                          : graded     ? graded_lane(k)
+                          : b->fine_priority ? b->fine_lanes[k] : b->lanes[k];
         VFS_CUDA(cudaStreamWaitEvent(fl, b->coarse_done[k], 0));
         if (k >= S) VFS_CUDA(cudaStreamWaitEvent(fl, b->fine_done[k - S], 0));
-        run(k, 2, S, fl, b->fine_priority >= 1);
+        run(k, 2, S, fl, coarse_first ? 0 : graded ? round_prio(k) : b->fine_priority >= 1 ? prio_hi : 0);
         VFS_CUDA(cudaEventRecord(b->fine_done[k], fl));
         if (io) pairs[k]->copyOutOn("u", io->u[k], io->device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, fl);
         VFS_CUDA(cudaEventRecord(b->lane_done[k], fl));
