@@ -226,8 +226,10 @@ int vfs_batch_set_fine_concurrency(vfs_batch* b, int max_pairs);
  * full-resolution parts on high-priority streams, priority = 2 also the first max_pairs
  * pairs' coarser levels, so that full-resolution work starts while the other pairs' coarse
  * levels run; priority = 3 runs all of pair k's work at the priority of its full-resolution
- * round k / max_pairs (the first round highest), so that each round's coarse levels fill the
- * gaps of the rounds before it.  Results are unchanged. */
+ * round k / max_pairs (the first round highest); priority = 4, the default, runs the coarser
+ * levels above the full-resolution levels (the first round's coarser levels highest), so that
+ * every pair's chain of small coarse launches advances while the full-resolution launches
+ * fill the rest of the GPU; 0 uses no priorities.  Results are unchanged. */
 int vfs_batch_set_pipeline(vfs_batch* b, int stagger_coarse, int priority);
 int vfs_set_autotune(vfs_stereo* s, int on);
 /* Force one variant of the fused iteration kernel at every pyramid level (-1: the tuned or

@@ -355,7 +355,8 @@ class StereoBatch:
     def set_pipeline(self, stagger_coarse: bool, priority: int) -> None:
         """With a full-resolution limit: stagger the coarse levels too; priority 1 runs the
         full-resolution parts on high-priority streams, 2 also the first pairs' coarse levels,
-        3 every part of pair k at the priority of its full-resolution round."""
+        3 every part of pair k at the priority of its full-resolution round, 4 (default) the
+        coarse levels above the full-resolution levels; 0 no priorities."""
         check_batch(self._h, self._L.vfs_batch_set_pipeline(self._h, int(stagger_coarse), int(priority)))
 
     def add(self, solver: "StereoTgv") -> None:
