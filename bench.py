@@ -528,9 +528,9 @@ def run_ours(args, rank, world, local):
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                          "limiter": "instruction issue and short dependencies with the working sets of the pairs "
-                                    "at full resolution resident in L2 (ncu, one cold launch: DRAM 20 %, issue 58 %, "
-                                    "251 warp instructions per 32 pixels; stalls per issued instruction: long "
-                                    "scoreboard 5.0, not selected 3.3, short scoreboard 2.7); frac > 1 is an "
+                                    "at full resolution resident in L2 (ncu, one cold launch: DRAM 24 %, issue 53 %, "
+                                    "228 warp instructions per 32 pixels; stalls per issued instruction: long "
+                                    "scoreboard 8.4, short scoreboard 3.1, not selected 2.1); frac > 1 is an "
                                     "algorithmic-bytes rate, not DRAM traffic",
                          "frac_in_mask": (achieved * in_mask_frac / peak) if achieved else None,
                          "frac_per_launch": (pi_l * b_alg / (ms_sum / 1000.0) / 1e9 / peak) if ms_sum > 0 else None,
