@@ -216,8 +216,9 @@ def cpu_baseline(pair, budget_s=12.0, precision=64):
 
 
 def run_reference(args, rank, world):
-    """--impl reference: the reference's solver restated on the host (the reference has no CPU
-    path of its own and its CUDA build cannot be compiled here), all host threads."""
+    """--impl reference: the reference's solver restated on the host cores, all host threads.
+    The reference has no CPU path of its own; its CUDA sources, built here as a test oracle
+    (oracle/_ref), run on the GPU and are compared with this library in the tests."""
     if rank != 0:
         return
     pair = pair_cache(W0, H0, args.seed)
