@@ -99,6 +99,11 @@ int vfs_import_state(vfs_stereo* s, const void* host, size_t bytes);
  * allocation of any handle fails as if the GPU were out of memory (the call returns
  * VFS_ERR_NOMEM and leaves nothing allocated); 0 turns it off. */
 int vfs_debug_fail_allocation(int n);
+/* Test hook (no counterpart in the reference): every device plane of a handle is followed by
+ * a 256-byte guard zone of 0xA5 bytes, written when the plane is allocated.  *bad_zones is the
+ * number of zones that no longer hold the pattern, i.e. that a kernel has stored into past the
+ * end of a plane (0 when every store stayed in bounds).  Synchronises the handle's stream. */
+int vfs_debug_check_guards(vfs_stereo* s, int* bad_zones);
 
 #define VFS_TENSOR_MATH_CUDA 0
 #define VFS_TENSOR_MATH_PORTABLE 1

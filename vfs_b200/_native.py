@@ -53,6 +53,7 @@ SIGNATURES = {
     "vfs_export_state": [_vp, _vp, _sz],
     "vfs_import_state": [_vp, _vp, _sz],
     "vfs_debug_fail_allocation": [_i],
+    "vfs_debug_check_guards": [_vp, ctypes.POINTER(ctypes.c_int)],
     "vfs_get_level_size": [_vp, _i, ctypes.POINTER(_i), ctypes.POINTER(_i), ctypes.POINTER(_i)],
     "vfs_load_vector_fields": [_vp, _vp, _vp],
     "vfs_copy_mask_to_device": [_vp, _vp],

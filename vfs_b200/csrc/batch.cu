@@ -98,6 +98,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
   // ---- levels -------------------------------------------------------------------------
   for (int level = maxL - 1; level >= 0; level--) {
     if ((part == 1 && level == 0) || (part == 2 && level > 0)) continue;
+    TraceRange trace(level_range_name(level));
     std::vector<StereoTgvImpl*> act;
     for (int k = 0; k < n; k++)
       if (level <= top[k]) act.push_back(pairs[k]);

@@ -240,6 +240,7 @@ int vfs_copy_mask_to_device(vfs_stereo* s, const float* mask) {
 }
 
 int vfs_copy_images_to_device_u8(vfs_stereo* s, const uint8_t* i0, const uint8_t* i1) {
+  vfs::TraceRange r("vfs_copy_images_to_device");
   return guarded(s, [&] { s->impl.copyImagesU8(i0, i1, false); });
 }
 
@@ -256,14 +257,24 @@ int vfs_copy_images_from_device_u8(vfs_stereo* s, const uint8_t* d0, const uint8
 }
 
 int vfs_solve_stereo_forward(vfs_stereo* s) {
+  vfs::TraceRange r("vfs_solve_stereo_forward");
   return guarded(s, [&] { s->impl.solve(false); });
 }
 
 int vfs_solve_stereo_forward_masked(vfs_stereo* s) {
+  vfs::TraceRange r("vfs_solve_stereo_forward_masked");
   return guarded(s, [&] { s->impl.solve(true); });
 }
 
+int vfs_debug_check_guards(vfs_stereo* s, int* bad_zones) {
+  return guarded(s, [&] {
+    if (!bad_zones) throw vfs::ArgError{"check guards: null output"};
+    *bad_zones = s->impl.checkGuards();
+  });
+}
+
 int vfs_copy_1d_disparity_to_host(vfs_stereo* s, float* u) {
+  vfs::TraceRange r("vfs_copy_1d_disparity_to_host");
   return guarded(s, [&] { s->impl.copyOut("u", u, true); });
 }
 
@@ -474,6 +485,7 @@ struct BatchHostIO {
 };
 
 void batch_solve(vfs_batch* b, int masked, const BatchHostIO* io) {
+  vfs::TraceRange trace("vfs_batch_solve");
   if (b->members.empty()) throw vfs::ArgError{"batch solve: empty batch"};
   std::vector<vfs::StereoTgvImpl*> pairs;
   for (auto* m : b->members) pairs.push_back(&m->impl);

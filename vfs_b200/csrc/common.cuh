@@ -1,6 +1,7 @@
 // Shared host/device helpers of the vfs_b200 library.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include <atomic>
@@ -33,6 +34,18 @@ std::atomic<long long>& launch_counter();
     VFS_CUDA(cudaGetLastError());                                           \
     ::vfs::launch_counter().fetch_add(1, std::memory_order_relaxed);        \
   } while (0)
+
+// Host-side trace ranges (NVTX) around the library's entry points and solve phases, for
+// profilers that record them (ncu --nvtx, Nsight Systems); without one attached they cost a
+// null check.  In graph replays a range covers the enqueue, not the GPU work.
+struct TraceRange {
+  explicit TraceRange(const char* name) { nvtxRangePushA(name); }
+  ~TraceRange() { nvtxRangePop(); }
+  TraceRange(const TraceRange&) = delete;
+  TraceRange& operator=(const TraceRange&) = delete;
+};
+// "level 0" .. "level 15"
+const char* level_range_name(int level);
 
 // Opt-in timing of launch groups with CUDA events on the solver's stream.
 struct ProfRec {

@@ -27,6 +27,13 @@ std::atomic<long long>& launch_counter() {
   return n;
 }
 
+const char* level_range_name(int level) {
+  static const char* names[16] = {"level 0",  "level 1",  "level 2",  "level 3", "level 4",  "level 5",
+                                  "level 6",  "level 7",  "level 8",  "level 9", "level 10", "level 11",
+                                  "level 12", "level 13", "level 14", "level 15"};
+  return names[level < 0 ? 0 : level > 15 ? 15 : level];
+}
+
 uint64_t next_generation() {
   static std::atomic<uint64_t> gen{0};
   return ++gen;
@@ -133,14 +140,36 @@ void StereoTgvImpl::release() {
   code_plain.clear();
   codes_valid = false;
   pool_bytes_ = pool_used_ = 0;
+  guards_.clear();
   initialized_ = false;
 }
 
 float* StereoTgvImpl::alloc(size_t bytes) {
   size_t off = (pool_used_ + 511) & ~(size_t)511;  // texture base alignment
-  if (off + bytes > pool_bytes_) throw ArgError{"internal: device pool overflow"};
-  pool_used_ = off + bytes;
+  if (off + bytes + kGuardBytes > pool_bytes_) throw ArgError{"internal: device pool overflow"};
+  pool_used_ = off + bytes + kGuardBytes;
+  guards_.push_back(pool_ + off + bytes);
   return (float*)(pool_ + off);
+}
+
+void StereoTgvImpl::fillGuards(size_t from, cudaStream_t st) {
+  for (size_t k = from; k < guards_.size(); k++) VFS_CUDA(cudaMemsetAsync(guards_[k], kGuardByte, kGuardBytes, st));
+}
+
+int StereoTgvImpl::checkGuards() {
+  if (guards_.empty()) return 0;
+  VFS_CUDA(cudaStreamSynchronize(stream_));
+  std::vector<unsigned char> h(kGuardBytes);
+  int bad = 0;
+  for (char* g : guards_) {
+    VFS_CUDA(cudaMemcpy(h.data(), g, kGuardBytes, cudaMemcpyDeviceToHost));
+    for (unsigned char c : h)
+      if (c != kGuardByte) {
+        bad++;
+        break;
+      }
+  }
+  return bad;
 }
 
 static int align_up(int n, int m) {
@@ -153,16 +182,18 @@ static int align_up(int n, int m) {
 // image staging; 512 B alignment slack per buffer.
 static size_t pool_bytes_for(const std::vector<int>& pS, const std::vector<int>& pH, size_t full) {
   size_t bytes = 0;
-  for (size_t l = 0; l < pS.size(); l++) bytes += (size_t)pS[l] * pH[l] * sizeof(float) * 5 + 4 * 512;
+  for (size_t l = 0; l < pS.size(); l++)
+    bytes += (size_t)pS[l] * pH[l] * sizeof(float) * 5 + 4 * 512 + 4 * StereoTgvImpl::kGuardBytes;
   const size_t planes = 18 + 10 * 2 + 4 + 2 * 3 + 4;
-  return bytes + full * sizeof(float) * planes + full * (2 + 2 * 3) + 64 * 512;
+  return bytes + full * sizeof(float) * planes + full * (2 + 2 * 3) + 64 * 512 + 40 * StereoTgvImpl::kGuardBytes;
 }
 
 // p, q two planes each (float: 8 + 16 bytes per pixel and plane), half v-bar pair, and
 // two edge-code bytes per pixel and level.
 static size_t fused_bytes_for(const std::vector<int>& pS, const std::vector<int>& pH, size_t full) {
-  size_t bytes = full * 2 * 8 + full * 2 * 16 + full * 4 * 2 + full * 16 + full * 8 + 8 * 512;
-  for (size_t l = 0; l < pS.size(); l++) bytes += 2 * ((size_t)pS[l] * pH[l] + 512);
+  size_t bytes = full * 2 * 8 + full * 2 * 16 + full * 4 * 2 + full * 16 + full * 8 + 8 * 512 +
+                 8 * StereoTgvImpl::kGuardBytes;
+  for (size_t l = 0; l < pS.size(); l++) bytes += 2 * ((size_t)pS[l] * pH[l] + 512 + StereoTgvImpl::kGuardBytes);
   return bytes;
 }
 
@@ -278,6 +309,7 @@ void StereoTgvImpl::initialize(const SolverParams& p) {
   // The reference leaves its buffers uninitialised after cudaMalloc; this
   // implementation starts from all-zero state so that results are deterministic.
   VFS_CUDA(cudaMemsetAsync(pool_, 0, pool_bytes_, stream_));
+  fillGuards(0, stream_);
   VFS_CUDA(cudaStreamSynchronize(stream_));
   initialized_ = true;
 }
@@ -391,10 +423,14 @@ void StereoTgvImpl::ensureFused() {
     throw CudaError{e, "cudaMalloc(fused buffers)", __FILE__, __LINE__};
   }
   size_t off = 0;
+  const size_t guards_before = guards_.size();
   auto take = [&](size_t b) {
     off = (off + 511) & ~(size_t)511;
+    if (off + b + kGuardBytes > bytes) throw ArgError{"internal: fused pool overflow"};
     char* p = fpool_ + off;
     off += b;
+    guards_.push_back(fpool_ + off);
+    off += kGuardBytes;
     return p;
   };
   f_p = take(n * 2 * 8);
@@ -410,6 +446,7 @@ void StereoTgvImpl::ensureFused() {
     code_plain[l] = (uint8_t*)take((size_t)pS[l] * pH[l]);
   }
   VFS_CUDA(cudaMemsetAsync(fpool_, 0, bytes, stream_));
+  fillGuards(guards_before, stream_);
   for (int l = 0; l < levels(); l++) launch_edge_codes(nullptr, code_plain[l], pW[l], pH[l], pS[l], stream_);
   codes_valid = false;
 }
@@ -429,6 +466,7 @@ void StereoTgvImpl::solveReference(bool masked) {
     launch_downscale(t1(pI1[l - 1], l - 1), 1, pI1[l], geom(l), st);
   }
   for (int level = top; level >= 0; level--) {
+    TraceRange trace(level_range_name(level));
     Geom g = geom(level);
     const float* mk = masked ? pMask[level] : nullptr;
     for (float* b : {d_a, d_b, d_c, d_etau, d_etav1, d_etav2, d_i0smooth}) VFS_CUDA(cudaMemsetAsync(b, 0, f, st));

@@ -212,6 +212,12 @@ class StereoTgvImpl {
   float* d_pack = nullptr;  // tight staging for device-to-host copies
 
   size_t pool_bytes() const { return pool_bytes_; }
+  // Guard zones: kGuardBytes of kGuardByte after every device plane of both pools, written at
+  // allocation; checkGuards() counts the zones a kernel has written into (out-of-bounds
+  // stores), vfs_debug_check_guards in the C ABI.
+  static constexpr size_t kGuardBytes = 256;
+  static constexpr unsigned char kGuardByte = 0xA5;
+  int checkGuards();
   TexCache tex;
 
   // ---- opt-in event timing of launch groups (bench / profiling) -----------
@@ -231,6 +237,8 @@ class StereoTgvImpl {
  private:
   void release();
   float* alloc(size_t bytes);
+  void fillGuards(size_t from, cudaStream_t st);
+  std::vector<char*> guards_;
   Geom geom(int level) const { return Geom{pW[level], pH[level], pS[level]}; }
   cudaTextureObject_t t1(const float* p, int level, bool linear = true) {
     return tex.get(p, pW[level], pH[level], (size_t)pS[level] * sizeof(float), 1, linear);

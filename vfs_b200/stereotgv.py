@@ -108,6 +108,13 @@ class StereoTgv:
     def synchronize(self) -> None:
         check(self._h, self._L.vfs_synchronize(self._h))
 
+    def check_guards(self) -> int:
+        """Number of the guard zones after the handle's device planes that a kernel has
+        stored into (0: every store stayed in bounds)."""
+        n = ctypes.c_int(-1)
+        check(self._h, self._L.vfs_debug_check_guards(self._h, ctypes.byref(n)))
+        return n.value
+
     def set_solve_path(self, fused: bool, half_storage: bool = False) -> None:
         """Select the drop-in path (one kernel per reference kernel) or the fused path
         (optionally with p, q, v-bar stored as half)."""
