@@ -42,7 +42,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--path", default="fused", choices=["fused", "plain"])
     ap.add_argument("--batch", type=int, default=0, help="pairs per rank (default: 8 fused, 1 plain)")
-    ap.add_argument("--storage", default="fp16", choices=["fp16", "fp32"], help="fused path: p, q, v-bar storage")
+    ap.add_argument("--storage", default="fp16", choices=["fp16", "fp32"], help="fused path: p, q, v-bar and warped-image storage")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain drop-in comparison run")
     ap.add_argument("--seed", type=int, default=20260)
     ap.add_argument("--mode", default="frames", choices=["frames", "mixed", "serving"],

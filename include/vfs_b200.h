@@ -158,8 +158,9 @@ int vfs_debug_get_buffer(vfs_stereo* s, const char* name, int comps, float* out)
  *   VFS_PATH_REFERENCE: one kernel per reference kernel, in the reference's order;
  *   VFS_PATH_FUSED: one fused kernel per primal-dual iteration plus fused per-warp and
  *   per-level kernels, replayed as a CUDA graph.  With float storage the fused path gives
- *   bit-identical results; with half storage (half_storage = 1) p, q and v-bar are kept
- *   as IEEE half in memory (all arithmetic stays float). */
+ *   bit-identical results; with half storage (half_storage = 1) p, q, v-bar and the warped
+ *   image are kept as IEEE half in memory (all arithmetic stays float; the warped image is
+ *   widened to float when it is copied out). */
 #define VFS_PATH_REFERENCE 0
 #define VFS_PATH_FUSED 1
 int vfs_set_solve_path(vfs_stereo* s, int path, int half_storage);

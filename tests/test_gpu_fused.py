@@ -110,6 +110,16 @@ def test_half_storage_accuracy(gpu):
     d = np.abs(u.astype(np.float64) - o.get("u"))[m]
     assert d.mean() <= 0.05, d.mean()
     assert (d > 1.0).mean() < 0.01
+    # the warped image is stored in half: copyWarpedImageToHost widens exactly representable
+    # half values, close to the float form's warped image of the same frame
+    w16 = s.copyWarpedImageToHost()
+    assert np.isfinite(w16).all()
+    assert np.array_equal(w16.astype(np.float16).astype(np.float32), w16)
+    assert np.array_equal(s.debug_buffer("i1warp", 1), w16)
+    f = make(pair.i0, pair.i1, pair.mask, pair.tv, pair.cv, p, fused=True, half=False)
+    solve_frames(f, pair.i0, pair.i1, True, 1)
+    dw = np.abs(w16 - f.copyWarpedImageToHost())[m]
+    assert dw.mean() <= 2e-3, dw.mean()
 
 
 @pytest.mark.parametrize("one_launch", [False, True])

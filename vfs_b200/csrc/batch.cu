@@ -169,7 +169,7 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
           StereoTgvImpl* s = act[k];
           DerivPair& d = Dv.pr[k];
           d.texI0 = s->tex1(s->pI0[level], level);
-          d.texI1w = s->tex1(s->d_i1warp, level);
+          d.texI1w = half ? s->tex1h(s->d_i1warp, level) : s->tex1(s->d_i1warp, level);
           d.tv = s->pTvF[level];
           d.Iu = s->d_Iu;
           d.Iz = s->d_Iz;
@@ -692,6 +692,7 @@ void FusedEngine::prepare(std::vector<StereoTgvImpl*>& pairs, bool masked) {
 
 void FusedEngine::solve(std::vector<StereoTgvImpl*>& pairs, bool masked, bool half, cudaStream_t st, int part) {
   solve_parts(pairs, masked, half, st, part);
+  for (auto* s : pairs) s->i1warp_half = half;
   if (part != 1)
     for (auto* s : pairs) s->have_prev = true;  // the frame's disparity is in d_u (warm starts)
 }

@@ -1,5 +1,6 @@
 // Shared host/device helpers of the vfs_b200 library.
 #pragma once
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
@@ -121,12 +122,15 @@ inline dim3 grid2d(int w, int h) { return dim3(iDivUp(w, kBX), iDivUp(h, kBY)); 
 inline dim3 block2d() { return dim3(kBX, kBY); }
 
 // Texture objects with the sampling setup of every gather of the reference
-// (normalized coordinates, mirror addressing, pitch-2D float / float2 memory).
-// Objects are created once per (pointer, geometry, filter) and kept for the life
-// of the cache, so a launch never creates or destroys one.
+// (normalized coordinates, mirror addressing, pitch-2D float / float2 memory, or one
+// half per texel for the FP16 form's warped image, read back as float).
+// Objects are created once per (pointer, geometry, filter, element) and kept for the
+// life of the cache, so a launch never creates or destroys one.
 class TexCache {
  public:
   ~TexCache() { clear(); }
+  // comps: 1 float, 2 float2, kHalf1 one half per texel
+  static constexpr int kHalf1 = -1;
   cudaTextureObject_t get(const void* ptr, int w, int h, size_t pitchBytes, int comps, bool linear) {
     Key k{(uintptr_t)ptr, w, h, pitchBytes, comps, linear};
     auto it = map_.find(k);
@@ -134,7 +138,9 @@ class TexCache {
     cudaResourceDesc rd = {};
     rd.resType = cudaResourceTypePitch2D;
     rd.res.pitch2D.devPtr = const_cast<void*>(ptr);
-    rd.res.pitch2D.desc = comps == 2 ? cudaCreateChannelDesc<float2>() : cudaCreateChannelDesc<float>();
+    rd.res.pitch2D.desc = comps == 2        ? cudaCreateChannelDesc<float2>()
+                          : comps == kHalf1 ? cudaCreateChannelDescHalf()
+                                            : cudaCreateChannelDesc<float>();
     rd.res.pitch2D.width = w;
     rd.res.pitch2D.height = h;
     rd.res.pitch2D.pitchInBytes = pitchBytes;

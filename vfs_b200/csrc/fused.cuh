@@ -181,7 +181,7 @@ struct WarpStartPair {
   cudaTextureObject_t texI1, texTv;
   const float2* warpUV;
   float2* tv2;
-  float* i1warp;
+  void* i1warp;  // warped image: float, or half with half_storage
   void *p, *q, *v_;  // zeroed (px < w); storage type by half_storage
   int w, h, s, tiles_x, tile0;
 };
@@ -193,7 +193,7 @@ void launch_warp_start(const WarpStartArgs& A, bool half_storage, cudaStream_t s
 
 // ---- derivatives along the translation field + u_last = u -----------------------
 struct DerivPair {
-  cudaTextureObject_t texI0, texI1w;
+  cudaTextureObject_t texI0, texI1w;  // texI1w over the warped image as stored (float or half)
   const float2* tv;
   float *Iu, *Iz;
   const float* u;

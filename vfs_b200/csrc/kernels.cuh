@@ -18,6 +18,7 @@ void launch_cv8u_to_gray(const uint8_t* src, float* dst, Geom g, cudaStream_t st
 void launch_cv8uc3_to_gray(const uchar3* src, float* dst, Geom g, cudaStream_t st);
 void launch_cv8u_tight_to_gray2(const uint8_t* s0, const uint8_t* s1, float* d0, float* d1, Geom g, cudaStream_t st);
 void launch_pack_tight(const float* src, float* dst, int comps, Geom g, cudaStream_t st);
+void launch_pack_tight_half(const void* src, float* dst, Geom g, cudaStream_t st);
 // downscale.cu:10-30 (float) / :98-122 (float2): mean of 4 taps at +-1/4 coarse px
 void launch_downscale(cudaTextureObject_t fine, int comps, float* out, Geom coarse, cudaStream_t st);
 // downscale.cu:52-73 point-sampled (mask pyramid)

@@ -399,7 +399,8 @@ void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, c
 
 // ---------------------------------------------------------------------------
 // Per-warp prologue: zero p, q (both halves) and v-bar; tv2 = tv(x + warpUV);
-// i1warp = I1(x + warpUV)  (stereotgv.cu:431-439; warpImage.cu:9-23, 96-111)
+// i1warp = I1(x + warpUV)  (stereotgv.cu:431-439; warpImage.cu:9-23, 96-111), stored in
+// the storage type (rounded to half with half storage)
 // ---------------------------------------------------------------------------
 template <class ST>
 __global__ void __launch_bounds__(kFTW* kFTH) k_warp_start(const __grid_constant__ WarpStartArgs A) {
@@ -419,7 +420,7 @@ __global__ void __launch_bounds__(kFTW* kFTH) k_warp_start(const __grid_constant
   float x = ((float)ix + wv.x + 0.5f) / (float)P.w;
   float y = ((float)iy + wv.y + 0.5f) / (float)P.h;
   P.tv2[pos] = tex2D<float2>(P.texTv, x, y);
-  P.i1warp[pos] = tex2D<float>(P.texI1, x, y);
+  ((ST*)P.i1warp)[pos] = (ST)tex2D<float>(P.texI1, x, y);
 }
 
 void launch_warp_start(const WarpStartArgs& A, bool half_storage, cudaStream_t st) {

@@ -51,6 +51,13 @@ __global__ void k_pack_tight(const float* src, float* dst, int comps, Geom g) {
   for (int c = 0; c < comps; c++) dst[di + c] = src[si + c];
 }
 
+// A pitched half plane (the FP16 form's warped image) widened to float into a tight buffer.
+__global__ void k_pack_tight_half(const __half* src, float* dst, Geom g) {
+  int ix, iy;
+  if (!pixel(ix, iy, g.w, g.h)) return;
+  dst[(long long)ix + (long long)g.w * iy] = __half2float(src[(long long)ix + (long long)g.s * iy]);
+}
+
 __global__ void k_cv8uc3_to_gray(const uchar3* src, float* dst, Geom g) {
   int ix, iy;
   if (!pixel(ix, iy, g.w, g.h)) return;
@@ -501,6 +508,10 @@ void launch_cv8u_tight_to_gray2(const uint8_t* s0, const uint8_t* s1, float* d0,
 }
 void launch_pack_tight(const float* src, float* dst, int comps, Geom g, cudaStream_t st) {
   k_pack_tight<<<L2D(g)>>>(src, dst, comps, g);
+  VFS_LAUNCH_CHECK();
+}
+void launch_pack_tight_half(const void* src, float* dst, Geom g, cudaStream_t st) {
+  k_pack_tight_half<<<L2D(g)>>>((const __half*)src, dst, g);
   VFS_LAUNCH_CHECK();
 }
 void launch_cv8uc3_to_gray(const uchar3* src, float* dst, Geom g, cudaStream_t st) {

@@ -456,6 +456,7 @@ void StereoTgvImpl::ensureFused() {
 // reference (stereotgv.cu:350-351 is commented out).
 void StereoTgvImpl::solveReference(bool masked) {
   cudaStream_t st = stream_;
+  i1warp_half = false;
   const size_t f = full_ * sizeof(float);
   launch_warp_image(t1(pI1[0], 0), d_cv, d_i1calibrated, geom(0), st);
   std::swap(pI1[0], d_i1calibrated);
@@ -538,7 +539,7 @@ struct StateHeader {
   uint32_t magic, version;
   int32_t width, height, stride, levels, stride_alignment, has_fused;
   float fScale;
-  int32_t f_parity, have_prev, reserved;
+  int32_t f_parity, have_prev, i1warp_half;
   uint64_t pool_bytes, fpool_bytes;
   int64_t role[kStateRoles];  // byte offsets in their pool (the last two: the fused pool); -1 = null
 };
@@ -567,6 +568,7 @@ void StereoTgvImpl::exportState(void* host, size_t bytes) {
   h.fScale = P.fScale;
   h.f_parity = f_parity;
   h.have_prev = have_prev ? 1 : 0;
+  h.i1warp_half = i1warp_half ? 1 : 0;
   h.pool_bytes = pool_bytes_;
   h.fpool_bytes = fbytes;
   const void* roles[kStateRoles] = {pI1[0], d_i1calibrated, d_u, d_us, d_u_, d_u_s,
@@ -624,6 +626,7 @@ void StereoTgvImpl::importState(const void* host, size_t bytes) {
   }
   f_parity = h.f_parity;
   have_prev = h.have_prev != 0;
+  i1warp_half = h.i1warp_half != 0;
   codes_valid = false;  // the masked edge codes and tile spans are derived again from the mask
   generation = next_generation();
 }
@@ -646,6 +649,14 @@ void StereoTgvImpl::copyOutOn(const char* what, float* dst, cudaMemcpyKind kind,
   else if (!std::strcmp(what, "X")) { src = d_X; comps = 3; }
   else if (!std::strcmp(what, "rgb")) { src = d_uvrgb; comps = 3; }
   else throw ArgError{std::string("copy: unknown buffer ") + what};
+  if (src == d_i1warp && i1warp_half) {
+    // the FP16 form's warped image: widened to float on the device, tight rows either way
+    float* out = kind == cudaMemcpyDeviceToHost ? d_pack : dst;
+    launch_pack_tight_half(src, out, geom(0), st);
+    if (kind == cudaMemcpyDeviceToHost)
+      VFS_CUDA(cudaMemcpyAsync(dst, d_pack, (size_t)width * height * sizeof(float), kind, st));
+    return;
+  }
   if (kind == cudaMemcpyDeviceToHost) {
     // pack on the device, then one contiguous download
     launch_pack_tight((const float*)src, d_pack, comps, geom(0), st);
@@ -680,6 +691,11 @@ void StereoTgvImpl::debugGet(const char* name, int comps, float* out) {
              {"v_", d_v_, 2},        {"Tp", d_Tp, 2},         {"us", d_us, 1},         {"u_s", d_u_s, 1},
              {"v_s", d_v_s, 2},      {"du", d_du, 1},         {"u_last", d_u_last, 1}, {"X", d_X, 3},
              {"depth", d_depth, 1},  {"warpUVs", d_warpUVs, 2}, {"i1calibrated", d_i1calibrated, 1}};
+  if (!std::strcmp(name, "i1warp") && i1warp_half) {  // half values: widened by copyOut
+    if (comps != 1) throw ArgError{"debug get: component count mismatch"};
+    copyOut("i1warp", out, true);
+    return;
+  }
   for (auto& e : tab) {
     if (std::strcmp(e.n, name)) continue;
     if (comps != e.c) throw ArgError{"debug get: component count mismatch"};

@@ -156,7 +156,10 @@ class StereoTgvImpl {
   int width = 0, height = 0, stride = 0;
   std::vector<int> pW, pH, pS;
   SolvePath path = SolvePath::kReference;
-  bool half_storage = false;  // fused path: p, q, v-bar stored as half
+  bool half_storage = false;  // fused path: p, q, v-bar and the warped image stored as half
+  // d_i1warp holds half values at the level-0 stride (the last solve was the fused path with
+  // half storage); copies of the warped image widen them to float
+  bool i1warp_half = false;
   std::string last_error;
 
   // ---- fused-path state (allocated on first use) ------------------------------
@@ -191,6 +194,10 @@ class StereoTgvImpl {
   Geom geomAt(int level) const { return Geom{pW[level], pH[level], pS[level]}; }
   cudaTextureObject_t tex1(const float* p, int level, bool linear = true) { return t1(p, level, linear); }
   cudaTextureObject_t tex2(const float2* p, int level) { return t2(p, level); }
+  // a plane holding one half per pixel at the level's stride (linear filtering)
+  cudaTextureObject_t tex1h(const void* p, int level) {
+    return tex.get(p, pW[level], pH[level], (size_t)pS[level] * sizeof(__half), TexCache::kHalf1, true);
+  }
   size_t fullElems() const { return full_; }
 
   // ---- device state (names follow stereotgv.h:48-96) ------------------------

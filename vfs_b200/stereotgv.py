@@ -117,7 +117,7 @@ class StereoTgv:
 
     def set_solve_path(self, fused: bool, half_storage: bool = False) -> None:
         """Select the drop-in path (one kernel per reference kernel) or the fused path
-        (optionally with p, q, v-bar stored as half)."""
+        (optionally with p, q, v-bar and the warped image stored as half)."""
         check(self._h, self._L.vfs_set_solve_path(self._h, PATH_FUSED if fused else PATH_REFERENCE,
                                                   int(half_storage)))
 
