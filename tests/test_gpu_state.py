@@ -95,6 +95,8 @@ def test_export_import_continues_bit_for_bit(gpu, fused, half):
                  p["f_scale"], p["n_warp"], p["n_iter"])
     b.set_warm_start(1)
     b.import_state(st)
+    # the imported warped image reads back as exported (half values widened in the FP16 form)
+    assert np.array_equal(a.copyWarpedImageToHost(), b.copyWarpedImageToHost())
     for s in (a, b):
         s.copyImagesToDevice(*frames[2])
         s.solveStereoForwardMasked()
