@@ -268,20 +268,27 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def fp64_u(pair):
-    """One float64 oracle solve of a pair (all host threads)."""
+def fp64_u(pair, w=W0, h=H0):
+    """One float64 oracle solve of a w x h pair (all host threads)."""
     from oracle.oracle import OracleStereoTgv
     from vfs_b200 import synth
     sp = synth.SOLVER_PARAMS
     o = OracleStereoTgv(64)
     o.set_limit_range(synth.LIMIT_RANGE)
-    o.initialize(W0, H0, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"], sp["lambda_"],
-                 synth.n_levels_for(W0), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+    o.initialize(w, h, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"], sp["lambda_"],
+                 synth.n_levels_for(w), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
     o.copy_mask_to_device(pair["mask"])
     o.load_vector_fields(pair["tv"], pair["cv"])
     o.copy_images_to_device(pair["i0"], pair["i1"])
     o.solve_stereo_forward_masked()
     return o.get("u")
+
+
+def error_stats(us, refs, masks):
+    """Disparity error of the solves `us` against float64 oracle solves `refs`, inside the masks."""
+    d = np.concatenate([np.abs(np.asarray(u, np.float64) - r)[m > 0] for u, r, m in zip(us, refs, masks)])
+    return {"mean_abs_px": float(d.mean()), "max_abs_px": float(d.max()), "bad_1px_rate": float((d > 1.0).mean()),
+            "frames": len(us)}
 
 
 def accuracy_report(pairs, u_timed, u64_first, half, dev):
@@ -571,8 +578,8 @@ def run_ours(args, rank, world, local):
             # the metric's other configurations, run after the timed region on the same GPU
             mixed = run_mixed(args, emit=False)
             result["mixed_batch"] = {k: mixed[k] for k in ("value", "unit", "ms_per_step", "latency_ms",
-                                                            "max_abs_vs_plain_px", "one_launch_per_level",
-                                                            "config")}
+                                                            "max_abs_vs_plain_px", "accuracy_vs_fp64_oracle",
+                                                            "one_launch_per_level", "config")}
             srv = run_serving(args, emit=False, local=local)
             result["serving"] = dict(srv["serving"], config=srv["config"])
             result["warm_start"] = warm_start_report(args.seed)
@@ -641,8 +648,10 @@ def run_mixed(args, emit=True):
     batch.set_mode(True)
     ms_one = time_steps()
     batch.set_mode(False)
-    # parity per size class: one more frame, against the drop-in path on a fresh handle pair
+    # parity per size class: one more frame, against the drop-in path on a fresh handle pair,
+    # and the error of both against the float64 oracle
     worst = 0.0
+    acc = {}
     for k in (0, 8, 12):
         w, h = sizes[k]
         ref = StereoTgv()
@@ -663,7 +672,9 @@ def run_mixed(args, emit=True):
         # the batch member has solved warmup + steps frames; solve a fresh fused handle once
         mine.copyImagesToDevice(pairs[k]["i0"], pairs[k]["i1"])
         mine.solveStereoForwardMasked()
-        worst = max(worst, float(np.abs(ref.copy1DDisparityToHost() - mine.copy1DDisparityToHost()).max()))
+        u_mine = mine.copy1DDisparityToHost()
+        worst = max(worst, float(np.abs(ref.copy1DDisparityToHost() - u_mine).max()))
+        acc["%dx%d" % (w, h)] = error_stats([u_mine], [fp64_u(pairs[k], w, h)], [pairs[k]["mask"]])
     per_step = float(np.mean(ms))
     line = {
         "metric": "mixed-size stereo frames/s (one batched fused solve per step)", "value": 16000.0 / per_step,
@@ -674,6 +685,8 @@ def run_mixed(args, emit=True):
                    "full_resolution_pairs_at_once": "auto" if args.fine < 0 else args.fine},
         "latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
         "max_abs_vs_plain_px": worst,
+        "accuracy_vs_fp64_oracle": dict(acc, sample="the first pair of each size, one frame, fused FP32 (the "
+                                        "drop-in path's bits); pixels inside the mask"),
         "one_launch_per_level": {"value": 16000.0 / float(np.mean(ms_one)), "unit": "frames/s",
                                  "ms_per_step": float(np.mean(ms_one)),
                                  "p99_ms": float(np.percentile(ms_one, 99))},
@@ -760,6 +773,7 @@ def run_serving(args, emit=True, rank=0, world=1, local=0):
     sp = synth.SOLVER_PARAMS
     params = dict(sp, limitRange=synth.LIMIT_RANGE)
     out = {}
+    u64 = {}  # float64 oracle solves of the sampled frames, shared by both servers
     for label, kw in (("fused_fp16_batched", dict(path="fused", half_storage=True, max_batch=8, lanes=2)),
                       ("plain_fp32_one_at_a_time", dict(path="plain"))):
         srv = StereoServer(reserve_bytes=1 << 30, **kw)
@@ -775,8 +789,27 @@ def run_serving(args, emit=True, rank=0, world=1, local=0):
         if world > 1:
             torch.distributed.barrier()  # the ranks start their replays together
         t_start = time.perf_counter()
-        replay(srv, sched, {sid: d[3] for sid, d in data.items()}, realtime=True)
+        reqs = replay(srv, sched, {sid: d[3] for sid, d in data.items()}, realtime=True)
         st = srv.stats(since=t_start)
+        # error against the float64 oracle on a sample: each stream's last frame (cold starts,
+        # so a frame's disparity depends on that frame alone)
+        last = {}
+        for r in reqs:
+            if r.u is not None and not r.cancelled and (r.stream_id not in last or r.seq > last[r.stream_id].seq):
+                last[r.stream_id] = r
+        us, refs, masks = [], [], []
+        for sid, r in sorted(last.items()):
+            w, h, fields, frames = data[sid]
+            key = (sid, r.seq)
+            if key not in u64:
+                u64[key] = fp64_u(dict(i0=r.i0, i1=r.i1, mask=fields["mask"], tv=fields["tv"], cv=fields["cv"]), w, h)
+            us.append(r.u)
+            refs.append(u64[key])
+            masks.append(fields["mask"])
+        if us:
+            st["accuracy_vs_fp64_oracle"] = dict(error_stats(us, refs, masks),
+                                                 sample="the last frame of each stream this rank serves; "
+                                                        "pixels inside the mask")
         if world > 1:
             d = [r for r in srv.done if r.t_submit >= t_start]
             job = merge_serving([r.latency_ms for r in d], min((r.t_submit for r in d), default=0.0),
