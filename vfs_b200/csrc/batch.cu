@@ -140,29 +140,33 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
       launch_level_gaussian(L, st);
       launch_level_tensor(L, st);
     }
+    // the per-warp prologue's arguments (the current v-bar buffer is the one the iterations
+    // left current, so the same call serves a warp's start and the previous warp's epilogue)
+    auto warp_start_args = [&]() {
+      WarpStartArgs W{};
+      for (int k = 0; k < na; k++) {
+        StereoTgvImpl* s = act[k];
+        WarpStartPair& d = W.pr[k];
+        d.texI1 = s->tex1(s->pI1[level], level);
+        d.texTv = s->tex2(s->pTvF[level], level);
+        d.warpUV = s->d_warpUV;
+        d.tv2 = s->d_tv2;
+        d.i1warp = s->d_i1warp;
+        d.p = s->f_p;
+        d.q = s->f_q;
+        d.v_ = half ? s->f_vh : (void*)s->d_v_;
+        d.w = s->pW[level];
+        d.h = s->pH[level];
+        d.s = s->pS[level];
+        set_tiles(W, k, d.w, d.h);
+      }
+      W.npairs = na;
+      return W;
+    };
     for (int warpIter = 0; warpIter < P0.nWarpIters; warpIter++) {
       prof->profBeginPx(kProfPrologue, px_level, 1, st);
-      {
-        WarpStartArgs W{};
-        for (int k = 0; k < na; k++) {
-          StereoTgvImpl* s = act[k];
-          WarpStartPair& d = W.pr[k];
-          d.texI1 = s->tex1(s->pI1[level], level);
-          d.texTv = s->tex2(s->pTvF[level], level);
-          d.warpUV = s->d_warpUV;
-          d.tv2 = s->d_tv2;
-          d.i1warp = s->d_i1warp;
-          d.p = s->f_p;
-          d.q = s->f_q;
-          d.v_ = half ? s->f_vh : (void*)s->d_v_;
-          d.w = s->pW[level];
-          d.h = s->pH[level];
-          d.s = s->pS[level];
-          set_tiles(W, k, d.w, d.h);
-        }
-        W.npairs = na;
-        launch_warp_start(W, half, st);
-      }
+      // later warps' prologues run in the previous warp's epilogue launch
+      if (warpIter == 0) launch_warp_start(warp_start_args(), half, st);
       {
         DerivArgs Dv{};
         for (int k = 0; k < na; k++) {
@@ -451,7 +455,8 @@ void fused_solve_direct(std::vector<StereoTgvImpl*>& pairs, bool masked, bool ha
           set_tiles(E, k, d.w, d.h);
         }
         E.npairs = na;
-        launch_warp_epilogue_batched(E, st);
+        if (warpIter + 1 < P0.nWarpIters) launch_epilogue_warp_start(E, warp_start_args(), half, st);
+        else launch_warp_epilogue_batched(E, st);
         if (masked)
           for (auto* s : act) std::swap(s->d_u, s->d_us);
       }

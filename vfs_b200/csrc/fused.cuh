@@ -223,6 +223,8 @@ struct EpiArgs {
   EpiPair pr[kMaxPairs];
 };
 void launch_warp_epilogue_batched(const EpiArgs& A, cudaStream_t st);
+// the epilogue (A) and the next warp's prologue (B, same pairs and tiles) in one launch
+void launch_epilogue_warp_start(const EpiArgs& A, const WarpStartArgs& B, bool half_storage, cudaStream_t st);
 
 // ---- per-level setup: gaussian (+ zero where not computed), tensor (+ zero) -------
 struct LevelPair {

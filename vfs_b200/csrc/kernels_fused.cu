@@ -402,12 +402,10 @@ void launch_fused_iteration(const IterArgs& A, bool masked, bool half_storage, c
 // i1warp = I1(x + warpUV)  (stereotgv.cu:431-439; warpImage.cu:9-23, 96-111), stored in
 // the storage type (rounded to half with half storage)
 // ---------------------------------------------------------------------------
+// the prologue at one pixel of a pair (pos = ix + iy * s; warpUV already read)
 template <class ST>
-__global__ void __launch_bounds__(kFTW* kFTH) k_warp_start(const __grid_constant__ WarpStartArgs A) {
+__device__ __forceinline__ void warp_start_at(const WarpStartPair& P, int ix, int iy, long long pos, float2 wv) {
   typedef Store2<ST> S;
-  TILE_SETUP(A)
-  if (ix >= P.w || iy >= P.h) return;
-  long long pos = ix + (long long)iy * P.s;
   long long plane = (long long)P.s * P.h;
   typename S::T2* p = (typename S::T2*)P.p;
   typename S::T4* q = (typename S::T4*)P.q;
@@ -416,11 +414,18 @@ __global__ void __launch_bounds__(kFTW* kFTH) k_warp_start(const __grid_constant
   S::st4(q, pos, make_float4(0.f, 0.f, 0.f, 0.f));
   S::st4(q, pos + plane, make_float4(0.f, 0.f, 0.f, 0.f));
   S::st2((typename S::T2*)P.v_, pos, make_float2(0.f, 0.f));
-  float2 wv = P.warpUV[pos];
   float x = ((float)ix + wv.x + 0.5f) / (float)P.w;
   float y = ((float)iy + wv.y + 0.5f) / (float)P.h;
   P.tv2[pos] = tex2D<float2>(P.texTv, x, y);
   ((ST*)P.i1warp)[pos] = (ST)tex2D<float>(P.texI1, x, y);
+}
+
+template <class ST>
+__global__ void __launch_bounds__(kFTW* kFTH) k_warp_start(const __grid_constant__ WarpStartArgs A) {
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  long long pos = ix + (long long)iy * P.s;
+  warp_start_at<ST>(P, ix, iy, pos, P.warpUV[pos]);
 }
 
 void launch_warp_start(const WarpStartArgs& A, bool half_storage, cudaStream_t st) {
@@ -466,11 +471,9 @@ void launch_derivatives_batched(const DerivArgs& A, cudaStream_t st) {
 
 // stereotgv.cu:481-493: median (masked form), du = min(u - u_last, limit),
 // u = u_last + du, u-bar = u, warpUV += du * tv2
-__global__ void __launch_bounds__(kFTW* kFTH) k_epilogue_b(const __grid_constant__ EpiArgs A) {
-  TILE_SETUP(A)
-  if (ix >= P.w || iy >= P.h) return;
-  long long pos = ix + (long long)iy * P.s;
-  float m = A.median ? median5_at(P.u_in, ix, iy, P.w, P.h, P.s) : P.u_in[pos];
+// the epilogue at one pixel of a pair; returns the updated warpUV it stored
+__device__ __forceinline__ float2 epilogue_at(const EpiPair& P, bool median, int ix, int iy, long long pos) {
+  float m = median ? median5_at(P.u_in, ix, iy, P.w, P.h, P.s) : P.u_in[pos];
   float ul = P.u_last[pos];
   float d = m - ul;
   d = d > P.limitRange ? P.limitRange : d;
@@ -480,7 +483,38 @@ __global__ void __launch_bounds__(kFTW* kFTH) k_epilogue_b(const __grid_constant
   float2 t = P.tv2[pos];
   float2 dw = make_float2(d * t.x, d * t.y);
   float2 wv = P.warpUV[pos];
-  P.warpUV[pos] = make_float2(wv.x + dw.x, wv.y + dw.y);
+  wv = make_float2(wv.x + dw.x, wv.y + dw.y);
+  P.warpUV[pos] = wv;
+  return wv;
+}
+
+__global__ void __launch_bounds__(kFTW* kFTH) k_epilogue_b(const __grid_constant__ EpiArgs A) {
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  epilogue_at(P, A.median != 0, ix, iy, ix + (long long)iy * P.s);
+}
+
+// The epilogue of one warp and the prologue of the next in one launch: both touch only their
+// own pixel's warpUV, tv2 and warped image (the epilogue reads tv2 before the prologue
+// replaces it; the median reads u, which the prologue does not write), and the pairs' tiles
+// are the same in both argument sets.
+template <class ST>
+__global__ void __launch_bounds__(kFTW* kFTH) k_epilogue_warp_start(const __grid_constant__ EpiArgs A,
+                                                                   const __grid_constant__ WarpStartArgs B) {
+  TILE_SETUP(A)
+  if (ix >= P.w || iy >= P.h) return;
+  const long long pos = ix + (long long)iy * P.s;
+  const float2 wv = epilogue_at(P, A.median != 0, ix, iy, pos);
+  warp_start_at<ST>(B.pr[pi_], ix, iy, pos, wv);
+}
+
+void launch_epilogue_warp_start(const EpiArgs& A, const WarpStartArgs& B, bool half_storage, cudaStream_t st) {
+  if (A.ntiles <= 0) return;
+  if (B.npairs != A.npairs || B.ntiles != A.ntiles) throw ArgError{"epilogue and warp start tiles differ"};
+  dim3 blk(kFTW, kFTH);
+  if (half_storage) k_epilogue_warp_start<__half><<<A.ntiles, blk, 0, st>>>(A, B);
+  else k_epilogue_warp_start<float><<<A.ntiles, blk, 0, st>>>(A, B);
+  VFS_LAUNCH_CHECK();
 }
 
 void launch_warp_epilogue_batched(const EpiArgs& A, cudaStream_t st) {

@@ -7,7 +7,9 @@ unless --autotune 1, so the launch sequence is fixed).
                                     [--variant -1..18] [--variants 1,1,8,9,9]
 
 Launch order per frame: pyramid, then per level (coarse to fine) the level kernels and per
-warp the prologue, the fused iterations and the epilogue.  With the default iteration
+warp the prologue (k_warp_start, first warp of a level only), the derivatives, the fused
+iterations and the epilogue (k_epilogue_warp_start, which also runs the next warp's prologue,
+or k_epilogue_b after a level's last warp).  With the default iteration
 variant (or --variant 0..2) each warp has 50 one-iteration launches: in the concurrent mode
 each pair's solve is enqueued in turn (pair 0 first), so k_fused_iter launches 600..749 are
 pair 0's full-resolution iterations (one pair per launch); in the one-launch mode every
