@@ -215,6 +215,28 @@ def cpu_baseline(pair, budget_s=12.0, precision=64):
     return n / dt, threads, o.get("u"), n, dt
 
 
+def cpu_single_thread_s(pair, precision=64):
+    """Seconds for one 848x800 frame of the CPU oracle on one host thread (the same solve as
+    cpu_baseline, OpenMP limited to one thread, then restored)."""
+    from oracle.oracle import OracleStereoTgv, set_threads
+    from vfs_b200 import synth
+    sp = synth.SOLVER_PARAMS
+    o = OracleStereoTgv(precision)
+    o.set_limit_range(synth.LIMIT_RANGE)
+    o.initialize(W0, H0, sp["beta"], sp["gamma"], sp["alpha0"], sp["alpha1"], sp["timestep_lambda"], sp["lambda_"],
+                 synth.n_levels_for(W0), sp["fScale"], sp["nWarpIters"], sp["nSolverIters"])
+    o.copy_mask_to_device(pair["mask"])
+    o.load_vector_fields(pair["tv"], pair["cv"])
+    o.copy_images_to_device(pair["i0"], pair["i1"])
+    prev = set_threads(1)
+    try:
+        t0 = time.perf_counter()
+        o.solve_stereo_forward_masked()
+        return time.perf_counter() - t0
+    finally:
+        set_threads(prev)
+
+
 def run_reference(args, rank, world):
     """--impl reference: the reference's solver restated on the host cores, all host threads.
     The reference has no CPU path of its own; its CUDA sources, built here as a test oracle
@@ -572,6 +594,7 @@ def run_ours(args, rank, world, local):
             result["cpu_baseline"] = {"value": fps, "unit": "frames/s", "cores": threads, "kind": "port",
                                       "sample": f"{n} full 848x800 frame(s) in {dt:.1f} s, float64 oracle "
                                                 f"(CPU restatement of the reference solver), OpenMP over rows"}
+            result["cpu_baseline"]["single_thread_s_per_frame"] = cpu_single_thread_s(pairs[0])
             if fused:
                 result["accuracy_vs_fp64_oracle"] = accuracy_report(pairs, outs, u_cpu, half, dev)
         if fused and world == 1 and not args.no_extras:

@@ -39,6 +39,8 @@ def lib():
         L.oracle_create.argtypes = [i]
         L.oracle_destroy.argtypes = [vp]
         L.oracle_set_hw_texture.argtypes = [i]
+        L.oracle_set_threads.argtypes = [i]
+        L.oracle_set_threads.restype = i
         L.oracle_initialize.argtypes = [vp, i, i, f, f, f, f, f, f, i, f, i, i, f, i, i]
         L.oracle_set_limit_range.argtypes = [vp, f]
         L.oracle_load_vector_fields.argtypes = [vp, vp, vp]
@@ -74,6 +76,11 @@ def tex_sample(tex: np.ndarray, xy: np.ndarray, linear: bool) -> np.ndarray:
 
 def set_hw_texture(on: bool) -> None:
     lib().oracle_set_hw_texture(int(on))
+
+
+def set_threads(n: int) -> int:
+    """OpenMP threads of this thread's later oracle solves (n > 0); returns the previous count."""
+    return int(lib().oracle_set_threads(int(n)))
 
 
 class OracleStereoTgv:

@@ -29,6 +29,8 @@
 #include <cstring>
 #include <vector>
 
+#include <omp.h>
+
 namespace vfs_oracle {
 
 // ---------------------------------------------------------------------------
@@ -828,6 +830,13 @@ void* oracle_create(int precision) {
 }
 void oracle_destroy(void* hp) { delete (Handle*)hp; }
 void oracle_set_hw_texture(int on) { g_hw_texture = on; }
+// OpenMP threads of the calling thread's later solves (n > 0); returns the previous count, so
+// that a single-threaded timing can put it back
+int oracle_set_threads(int n) {
+  const int prev = omp_get_max_threads();
+  if (n > 0) omp_set_num_threads(n);
+  return prev;
+}
 
 int oracle_initialize(void* hp, int width, int height, float beta, float gamma, float alpha0, float alpha1,
                       float timestep_lambda, float lambda, int nLevels, float fScale, int nWarpIters,

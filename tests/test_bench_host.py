@@ -28,3 +28,14 @@ def test_error_stats_counts_only_pixels_inside_the_masks():
     assert st["max_abs_px"] == 2.5
     assert abs(st["mean_abs_px"] - (2.5 + 0.25) / n) < 1e-12
     assert abs(st["bad_1px_rate"] - 1.0 / n) < 1e-12
+
+
+def test_oracle_thread_count_is_set_and_restored():
+    """The CPU baseline's single-thread frame limits the oracle to one OpenMP thread and puts
+    the previous count back."""
+    from oracle.oracle import build, set_threads
+    build()
+    prev = set_threads(1)
+    assert prev >= 1
+    assert set_threads(prev) == 1
+    assert set_threads(0) == prev  # 0 leaves the count as it is
